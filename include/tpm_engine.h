@@ -1,0 +1,189 @@
+/*
+ * tpm_engine.h — C ABI of the B200 TreePM force engine.
+ *
+ * This is the drop-in boundary for the force evaluation of EUNHA's GOTPM
+ * build (kjhan0606/LagEunha). The engine replaces
+ *   void pmmain(SimParameters *, EvolFact)                 Cosmos/pmmain.c:390
+ *   void treecorrection(SimParameters *, DeterminedEvolFact *)
+ *                                                          Cosmos/treecorrection.c:225
+ *   void TreeMain(SimParameters *, DeterminedEvolFact *)   Cosmos/Treemain.h:19
+ *                                                          (GOTPM body Treemain.c:578-664)
+ * and their helpers psolver (Cosmos/psolver.c:13) and fda4 (Cosmos/fda4.c:31).
+ * Those take SimParameters; this ABI takes plain pointers and sizes instead,
+ * so a caller fills tpm_params from the SimParameters fields it already has
+ * (NX, THETA, RSPHERE, GRV_EPSILON, GRV_EFOLD: eunha.h:1033-1090) and hands
+ * over the particle array it already owns.
+ *
+ * Every entry point returns 0 on success or a negative TPM_E* code; the
+ * message of the last failure on the calling thread is tpm_last_error().
+ * (The reference exits on error: Cosmos/treecorrection.c:245-246.)
+ *
+ * One tpm_ctx owns one periodic box on one GPU and its own CUDA stream.
+ * Calls on one context are not re-entrant; distinct contexts may be used from
+ * distinct threads.
+ */
+#ifndef TPM_ENGINE_H
+#define TPM_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TPM_OK 0
+#define TPM_E_ARG (-1)      /* bad argument */
+#define TPM_E_NOMEM (-2)    /* device allocation failed */
+#define TPM_E_CUDA (-3)     /* CUDA runtime or launch failure */
+#define TPM_E_STATE (-4)    /* call out of order (e.g. forces before particles) */
+#define TPM_E_OVERFLOW (-5) /* a bounded device work queue or stack overflowed */
+#define TPM_E_NODEV (-6)    /* no usable CUDA device */
+
+/* ---- force laws ---- */
+/* TPM_LAW_REFERENCE: the reference's split. PM Green's function
+ *   -1/(pi n^2) exp(-n^2 (pi efold / N)^2) / N^3       (Cosmos/psolver.c:58-72)
+ * and the tabulated residual law of OST/Model4TreeForce.c:48-116 (PMFITPARA)
+ * cut at rsphere. TPM_LAW_GAUSSIAN: a Gaussian split of scale rs_split cells
+ * with the matching erfc short-range law and TSC-deconvolved Green's
+ * function (no counterpart in the reference; see tpm_params). */
+#define TPM_LAW_REFERENCE 0
+#define TPM_LAW_GAUSSIAN 1
+
+/* ---- which parts of the force ---- */
+#define TPM_PART_PM 1u
+#define TPM_PART_TREE 2u
+#define TPM_PART_ALL 3u
+
+/* ---- where a buffer lives ---- */
+#define TPM_MEM_HOST 0
+#define TPM_MEM_DEVICE 1
+
+typedef struct tpm_params {
+  int32_t n_mesh;   /* PM mesh cells per side, NX = NY = NZ (eunha.h:1090) */
+  int32_t law;      /* TPM_LAW_* */
+  float theta;      /* opening angle THETA (eunha.h:1076); reference default 0.3 */
+  float rsphere;    /* short-range cutoff RSPHERE in cells; default 4 */
+  float epsilon;    /* Plummer softening GRV_EPSILON in cells */
+  float efold;      /* PM split GRV_EFOLD (reference law); default 0.9 */
+  float rs_split;   /* Gaussian split scale in cells (TPM_LAW_GAUSSIAN only) */
+  float particle_mass; /* particle mass (TDM_MASS); reference runs use 1 */
+} tpm_params;
+
+typedef struct tpm_ctx tpm_ctx;
+
+/* Defaults of the reference's parameter file for the GOTPM build
+ * (Params/header.c:148-149,501-505,651-653): theta 0.3, rsphere 4,
+ * efold 0.9, epsilon 0.1, mass 1. */
+void tpm_default_params(tpm_params *p, int32_t n_mesh);
+
+const char *tpm_last_error(void);
+const char *tpm_version(void);
+
+/* Create a context on CUDA device `device` with capacity for up to np_max
+ * particles (device memory is reserved lazily and grown on demand). */
+int tpm_create(const tpm_params *params, int device, tpm_ctx **out);
+int tpm_destroy(tpm_ctx *ctx);
+int tpm_set_params(tpm_ctx *ctx, const tpm_params *params);
+int tpm_get_params(const tpm_ctx *ctx, tpm_params *out);
+
+/* ---- particle state ---- */
+
+/* Positions as uint32 fixed point per axis, AoS [np][3]:
+ * u = round(frac(x / N) * 2^32), x in cells. vel may be NULL (zeros). */
+int tpm_load_fixed(tpm_ctx *ctx, int64_t np, const uint32_t *pos, const float *vel, int mem);
+
+/* Positions in the reference's XYZDBL form (eunha.h:1212,1228-1232): an AoS
+ * array of records of `stride` bytes holding a uint64 Lagrangian index
+ * (top byte = flags) at byte offset off_indx, float x,y,z offsets at off_pos
+ * and float vx,vy,vz at off_vel (off_vel < 0: zero velocities).
+ * GOTPM dmparticletype: stride 32, offsets 0, 8, 20 (eunha.h:390-400);
+ * treedmparticletype: stride 40, offsets 8, 16, 28 (eunha.h:401-412). */
+int tpm_load_lagrangian(tpm_ctx *ctx, int64_t np, const void *particles, int64_t stride,
+                        int64_t off_indx, int64_t off_pos, int64_t off_vel, int mem);
+
+/* Evaluate the forces of `parts` (TPM_PART_*) on the loaded particles and
+ * keep them on the device. Reference units: F in cells with G = m = 1 carries
+ * the reference's 1/N^2 factor. */
+int tpm_compute_forces(tpm_ctx *ctx, unsigned parts);
+
+/* Copy the last forces out, AoS [np][3] float, in the caller's particle order. */
+int tpm_read_forces(tpm_ctx *ctx, float *out, int mem);
+
+/* v += fact2_pm * F_pm + fact2_tree * F_tree using the last forces
+ * (Cosmos/fda4.h:297-299; OST/ost.ver2.c:273-291). */
+int tpm_kick(tpm_ctx *ctx, float fact2_pm, float fact2_tree);
+
+/* Drift: x += v * pfact (cells), accumulated in FP64 into the fixed-point
+ * positions (Cosmos/stepevolv.c:38-113). */
+int tpm_drift(tpm_ctx *ctx, double pfact);
+
+int tpm_read_velocities(tpm_ctx *ctx, float *out, int mem);
+int tpm_read_positions(tpm_ctx *ctx, uint32_t *out, int mem);
+
+/* Write the velocities back into a record array of the tpm_load_lagrangian
+ * form (only the vx,vy,vz fields are touched). */
+int tpm_store_lagrangian_velocities(tpm_ctx *ctx, void *particles, int64_t stride, int64_t off_vel,
+                                    int mem);
+
+/* Wait for all work queued on the context's stream. */
+int tpm_sync(tpm_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t) so callers can order their own
+ * work against it. */
+void *tpm_stream(tpm_ctx *ctx);
+
+/* ---- drop-in forms of the reference entry points ---- */
+
+/* pmmain (Cosmos/pmmain.c:390-527) on a GOTPM dmparticletype array:
+ * v += fact2 * F_PM. fact2 is the one pmmain's fda4 picks from EvolFact for
+ * the current PMSTATUS (Cosmos/fda4.c:48-62). */
+int tpm_pmmain(tpm_ctx *ctx, void *dm_particles, int64_t np, float fact2);
+
+/* treecorrection (Cosmos/treecorrection.c:225-475) on a GOTPM
+ * treedmparticletype array: v += fact2 * F_tree, fact2 = EvolFactArr[0].fact2
+ * (treecorrection.c:227). */
+int tpm_treecorrection(tpm_ctx *ctx, void *treedm_particles, int64_t np, float fact2);
+
+/* The GOTPM TreeMain step (Cosmos/Treemain.c:578-664): theta follows the
+ * step schedule 0.3 (step < 10), 0.35 (< 20), 0.4 (< 60), 0.45 after
+ * (Treemain.c:598-601) and stays set on the context, then treecorrection. */
+int tpm_treemain(tpm_ctx *ctx, void *treedm_particles, int64_t np, float fact2, int stepcount);
+
+/* ---- diagnostics ---- */
+
+/* FP64 periodic Ewald force (reference units, Plummer softening epsilon on
+ * pairs inside the real-space cutoff) on nt target particles given by their
+ * caller-order indices; forces [nt][3] double written to out (host). */
+int tpm_ewald(tpm_ctx *ctx, int64_t nt, const int64_t *targets, double *out);
+
+/* Per-stage device times (ms) of the last tpm_compute_forces, in the order
+ * sort, deposit, fft, fda4, tree_build, tree_walk, finish; returns the
+ * number of stages written (<= n). */
+int tpm_stage_times(tpm_ctx *ctx, float *ms, int n);
+
+/* Counters of the last force evaluation: [0] tree nodes, [1] particle-
+ * particle interactions, [2] particle-node interactions, [3] walk groups. */
+int tpm_counters(tpm_ctx *ctx, int64_t *out, int n);
+
+/* Kernel launches issued by the last tpm_compute_forces. */
+int64_t tpm_launch_count(tpm_ctx *ctx);
+
+/* The spatial order of the last tpm_compute_forces: sorted 39-bit Morton
+ * keys and the permutation (sorted slot -> caller index), np entries each,
+ * host memory. Either pointer may be NULL. */
+int tpm_read_order(tpm_ctx *ctx, uint64_t *keys, uint32_t *perm);
+
+/* Mesh stages of the last PM evaluation, [z][y][x] n^3 floats, host memory:
+ * TPM_MESH_DENSITY is the TSC mass per cell (the reference folds the same
+ * mesh minus 1, Cosmos/pmmain.c:304), TPM_MESH_POTENTIAL the potential after
+ * the Green's function and the c2r (Cosmos/pmmain.c:492). */
+#define TPM_MESH_DENSITY 0
+#define TPM_MESH_POTENTIAL 1
+int tpm_read_mesh(tpm_ctx *ctx, int which, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TPM_ENGINE_H */

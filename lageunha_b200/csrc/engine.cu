@@ -1,0 +1,802 @@
+// TreePM force engine: context, orchestration and the C ABI of
+// include/tpm_engine.h.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tpm_engine.h"
+#include "engine_internal.cuh"
+
+namespace tpm {
+int ewald_force(const uint32_t *pos, int64_t np, int n, float eps, int64_t nt, const int64_t *targets_host,
+                double *out_host, cudaStream_t st);
+int64_t walk_stack_words();
+}  // namespace tpm
+
+using namespace tpm;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(e_ == cudaErrorMemoryAllocation ? TPM_E_NOMEM : TPM_E_CUDA, "%s: %s (%s:%d)", #call, \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                          \
+  } while (0)
+
+enum Stage { kStSort = 0, kStDeposit, kStFft, kStFda4, kStTreeBuild, kStTreeWalk, kStFinish, kNStages };
+
+struct tpm_ctx {
+  tpm_params prm;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[kNStages + 1];
+  bool timing = true;
+  // particles
+  int64_t np = 0, cap = 0;
+  uint32_t *pos = nullptr;
+  float *vel = nullptr;
+  uint64_t *key = nullptr, *key_alt = nullptr;
+  uint32_t *val = nullptr, *val_alt = nullptr;
+  uint32_t *perm = nullptr;  // sorted -> caller index (one of val/val_alt)
+  uint64_t *skey = nullptr;  // sorted keys (one of key/key_alt)
+  uint32_t *spos = nullptr;
+  float *fpm = nullptr, *ftree = nullptr;  // sorted order
+  float *fout = nullptr;                   // caller order scratch
+  void *stage = nullptr;                   // record staging for the Lagrangian layout
+  size_t stage_bytes = 0;
+  SortScratch ss;
+  // mesh
+  MeshGeom g;
+  FftPlan fp;
+  float *rho = nullptr;
+  float2 *spec = nullptr;
+  float *phi = nullptr;
+  CUtensorMap tmap;
+  uint32_t *tile_start = nullptr;
+  // tree
+  TreeBuffers tb;
+  uint32_t *cube_start = nullptr;
+  int64_t ncubes = 0;
+  LawTable law;
+  int law_n = -1;
+  float law_eps = -1, law_rs = -1, law_rsphere = -1;
+  int law_kind = -1;
+  uint32_t *err = nullptr;
+  // bookkeeping
+  unsigned parts_valid = 0;
+  float stage_ms[kNStages];
+  unsigned stage_mask = 0;
+  int64_t launches = 0;
+  int64_t counters[4] = {0, 0, 0, 0};
+};
+
+extern "C" {
+
+void tpm_default_params(tpm_params *p, int32_t n_mesh) {
+  p->n_mesh = n_mesh;
+  p->law = TPM_LAW_REFERENCE;
+  p->theta = 0.3f;
+  p->rsphere = 4.0f;
+  p->epsilon = 0.1f;
+  p->efold = 0.9f;
+  p->rs_split = 1.25f;
+  p->particle_mass = 1.0f;
+}
+
+const char *tpm_last_error(void) { return g_err.c_str(); }
+const char *tpm_version(void) { return "lageunha_b200 tpm_engine 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+static int check_params(const tpm_params *p) {
+  if (!p) return fail(TPM_E_ARG, "params is NULL");
+  if (p->n_mesh < 16 || p->n_mesh > 4096) return fail(TPM_E_ARG, "n_mesh %d outside [16, 4096]", p->n_mesh);
+  if (p->law != TPM_LAW_REFERENCE && p->law != TPM_LAW_GAUSSIAN) return fail(TPM_E_ARG, "unknown law %d", p->law);
+  if (!(p->theta > 0.f && p->theta < 1.f)) return fail(TPM_E_ARG, "theta %g outside (0,1)", p->theta);
+  if (!(p->rsphere > 0.f && p->rsphere <= 6.0f)) return fail(TPM_E_ARG, "rsphere %g outside (0, 6]", p->rsphere);
+  if (p->rsphere * 4.f >= (float)p->n_mesh) return fail(TPM_E_ARG, "rsphere %g too large for n_mesh %d", p->rsphere, p->n_mesh);
+  if (!(p->epsilon >= 0.f)) return fail(TPM_E_ARG, "epsilon %g < 0", p->epsilon);
+  if (p->law == TPM_LAW_GAUSSIAN && !(p->rs_split > 0.f)) return fail(TPM_E_ARG, "rs_split must be > 0");
+  if (!(p->particle_mass > 0.f)) return fail(TPM_E_ARG, "particle_mass must be > 0");
+  return 0;
+}
+
+// ------------------------------------------------------------------ law table
+// Residual short-range law f(r)/N^2 and the table of OST/Model4TreeForce.c:
+// diff[i] = {-f/r, -(f'r - f)/(2 r^3), -(f''r^2 - 3f'r + 3f)/(2 r^5)} at
+// r = i*6/4096 with central differences of step 0.1*delta, entry 0 copied
+// from entry 1, slope[i] = (diff[i+1]-diff[i])/delta, last entry zero
+// (Model4TreeForce.c:48-91).
+static const double kPmFit[8] = {1.0 / 256.0 / 256.0, 0.78224E+00, 0.37971E-06, -0.60338E+00,
+                                 -0.34419E-07, -0.39741E+01, -0.10607E+01, -0.38145E+00};
+
+static double law_f(int kind, double r, float eps, double rs, double LL) {
+  double soft = r / pow(r * r + (double)(eps * eps), 1.5);
+  double longr;
+  if (kind == TPM_LAW_REFERENCE) {
+    // PMFITPARA fit of the reference's PM force (Model4TreeForce.c:92-116)
+    const double *P = kPmFit;
+    double t = cosh(P[1] * r);
+    longr = 1.0 / (r * r) * tanh(P[1] * r) - P[1] / (t * t * r) - 2.0 * P[2] / P[0] * r * exp(P[3] * r * r) -
+            2.0 * P[2] * P[3] / P[0] * r * r * r * exp(P[3] * r * r) +
+            P[4] / P[0] * (1.0 + P[5] * r * r + P[6] * r * r * r * r) * exp(P[7] * r * r);
+  } else {
+    // force of a Gaussian-filtered point mass, filter exp(-k^2 rs^2)
+    double u = r / (2.0 * rs);
+    longr = (erf(u) - 2.0 * u / sqrt(M_PI) * exp(-u * u)) / (r * r);
+  }
+  return (soft - longr) / LL;
+}
+
+static int build_law(tpm_ctx *c) {
+  const tpm_params &p = c->prm;
+  if (c->law.t01 && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
+      c->law_rs == p.rs_split && c->law_rsphere == p.rsphere)
+    return 0;
+  const int NS = 4096;
+  const double range = 6.0;
+  float ran2nran = (float)(range / NS);
+  float invran = (float)(1.0 / ran2nran);
+  double LL = (double)p.n_mesh * (double)p.n_mesh;
+  double dr = ran2nran * 0.1;
+  std::vector<double> diff((NS + 1) * 3, 0.0), slope(NS * 3, 0.0);
+  for (int i = 1; i < NS; i++) {
+    double r = (double)i * ran2nran;
+    double fp = (law_f(p.law, r + dr, p.epsilon, p.rs_split, LL) - law_f(p.law, r - dr, p.epsilon, p.rs_split, LL)) / (dr + dr);
+    double fpp = (law_f(p.law, r + 2 * dr, p.epsilon, p.rs_split, LL) - 2 * law_f(p.law, r, p.epsilon, p.rs_split, LL) +
+                  law_f(p.law, r - 2 * dr, p.epsilon, p.rs_split, LL)) / (4 * dr * dr);
+    double fr = law_f(p.law, r, p.epsilon, p.rs_split, LL);
+    diff[3 * i + 0] = -(fr / r);
+    diff[3 * i + 1] = -(0.5 * (fp * r - fr) / r / r / r);
+    diff[3 * i + 2] = -(0.5 * (fpp * r * r - 3 * fp * r + 3 * fr) / r / r / r / r / r);
+  }
+  for (int i = 0; i < NS; i++)
+    for (int k = 0; k < 3; k++) slope[3 * i + k] = (diff[3 * (i + 1) + k] - diff[3 * i + k]) / ran2nran;
+  for (int k = 0; k < 3; k++) {
+    slope[k] = slope[3 + k];
+    diff[k] = diff[3 + k];
+    diff[3 * (NS - 1) + k] = 0;
+    slope[3 * (NS - 1) + k] = 0;
+  }
+  int entries = (int)(p.rsphere * invran) + 2;
+  if (entries > NS) entries = NS;
+  std::vector<float4> t01(entries);
+  std::vector<float2> t2(entries + 1);
+  for (int i = 0; i < entries; i++) {
+    t01[i] = make_float4((float)diff[3 * i], (float)slope[3 * i], (float)diff[3 * i + 1], (float)slope[3 * i + 1]);
+    t2[i] = make_float2((float)diff[3 * i + 2], (float)slope[3 * i + 2]);
+  }
+  if (c->law.t01) cudaFree(c->law.t01);
+  if (c->law.t2) cudaFree(c->law.t2);
+  c->law.t01 = nullptr;
+  c->law.t2 = nullptr;
+  CK(cudaMalloc(&c->law.t01, sizeof(float4) * entries));
+  CK(cudaMalloc(&c->law.t2, sizeof(float2) * (entries + 1)));
+  CK(cudaMemcpy(c->law.t01, t01.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->law.t2, t2.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
+  c->law.entries = entries;
+  c->law.delta = ran2nran;
+  c->law.inv_delta = invran;
+  c->law_n = p.n_mesh;
+  c->law_eps = p.epsilon;
+  c->law_kind = p.law;
+  c->law_rs = p.rs_split;
+  c->law_rsphere = p.rsphere;
+  return 0;
+}
+
+// ------------------------------------------------------------------ buffers
+static void free_mesh(tpm_ctx *c) {
+  if (c->rho) cudaFree(c->rho);
+  if (c->spec) cudaFree(c->spec);
+  if (c->phi) cudaFree(c->phi);
+  if (c->tile_start) cudaFree(c->tile_start);
+  if (c->cube_start) cudaFree(c->cube_start);
+  fft_plan_free(c->fp);
+  c->rho = nullptr;
+  c->spec = nullptr;
+  c->phi = nullptr;
+  c->tile_start = nullptr;
+  c->cube_start = nullptr;
+}
+
+static int alloc_mesh(tpm_ctx *c) {
+  free_mesh(c);
+  c->g = make_geom(c->prm.n_mesh);
+  const MeshGeom &g = c->g;
+  int64_t n3 = (int64_t)g.n * g.n * g.n;
+  CK(cudaMalloc(&c->rho, sizeof(float) * n3));
+  CK(cudaMalloc(&c->spec, sizeof(float2) * g.spec_elems));
+  CK(cudaMalloc(&c->phi, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  CK(cudaMemset(c->phi, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  uint32_t ntiles = 1u << (3 * (g.cbits - 3));
+  CK(cudaMalloc(&c->tile_start, sizeof(uint32_t) * (ntiles + 1)));
+  c->ncubes = 1ll << (3 * (g.cbits - 2));
+  CK(cudaMalloc(&c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
+  fft_plan_init(c->fp, g.n);
+  if (make_phi_tensor_map(g, c->phi, &c->tmap) != 0) return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static void free_particles(tpm_ctx *c) {
+  void *ps[] = {c->pos, c->vel, c->key, c->key_alt, c->val, c->val_alt, c->spos, c->fpm, c->ftree, c->fout,
+                c->ss.hist, c->tb.start, c->tb.count, c->tb.child, c->tb.nchild, c->tb.level, c->tb.geo,
+                c->tb.mom0, c->tb.mom1, c->tb.mom2, c->tb.tile_sum, c->tb.groups};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  c->pos = nullptr;
+  c->vel = nullptr;
+  c->key = c->key_alt = nullptr;
+  c->val = c->val_alt = nullptr;
+  c->spos = nullptr;
+  c->fpm = c->ftree = c->fout = nullptr;
+  c->ss.hist = nullptr;
+  c->tb.start = c->tb.count = c->tb.child = c->tb.nchild = nullptr;
+  c->tb.level = nullptr;
+  c->tb.geo = nullptr;
+  c->tb.mom0 = c->tb.mom1 = c->tb.mom2 = nullptr;
+  c->tb.tile_sum = nullptr;
+  c->tb.groups = nullptr;
+  c->cap = 0;
+}
+
+static int ensure_particles(tpm_ctx *c, int64_t np) {
+  if (np <= c->cap) return 0;
+  free_particles(c);
+  int64_t cap = np;
+  CK(cudaMalloc(&c->pos, sizeof(uint32_t) * 3 * cap));
+  CK(cudaMalloc(&c->vel, sizeof(float) * 3 * cap));
+  CK(cudaMalloc(&c->key, sizeof(uint64_t) * cap));
+  CK(cudaMalloc(&c->key_alt, sizeof(uint64_t) * cap));
+  CK(cudaMalloc(&c->val, sizeof(uint32_t) * cap));
+  CK(cudaMalloc(&c->val_alt, sizeof(uint32_t) * cap));
+  CK(cudaMalloc(&c->spos, sizeof(uint32_t) * 3 * cap));
+  CK(cudaMalloc(&c->fpm, sizeof(float) * 3 * cap));
+  CK(cudaMalloc(&c->ftree, sizeof(float) * 3 * cap));
+  CK(cudaMalloc(&c->fout, sizeof(float) * 3 * cap));
+  int64_t ntiles = sort_tiles(cap);
+  CK(cudaMalloc(&c->ss.hist, sizeof(uint32_t) * 256 * (ntiles + 1)));
+  c->ss.cap_tiles = ntiles;
+  // tree: every node holds >= 1 particle and every inner node >= 10, so the
+  // node count is bounded by the leaves (<= np) plus the inner nodes
+  int64_t cap_nodes = cap + cap / 4 + 64;
+  TreeBuffers &tb = c->tb;
+  tb.cap_nodes = cap_nodes;
+  CK(cudaMalloc(&tb.start, sizeof(uint32_t) * cap_nodes));
+  CK(cudaMalloc(&tb.count, sizeof(uint32_t) * cap_nodes));
+  CK(cudaMalloc(&tb.child, sizeof(uint32_t) * cap_nodes));
+  CK(cudaMalloc(&tb.nchild, sizeof(uint32_t) * cap_nodes));
+  CK(cudaMalloc(&tb.level, sizeof(uint8_t) * cap_nodes));
+  CK(cudaMalloc(&tb.geo, sizeof(uint4) * cap_nodes));
+  CK(cudaMalloc(&tb.mom0, sizeof(float4) * cap_nodes));
+  CK(cudaMalloc(&tb.mom1, sizeof(float4) * cap_nodes));
+  CK(cudaMalloc(&tb.mom2, sizeof(float4) * cap_nodes));
+  int64_t ts = (cap_nodes + 1023) / 1024 + 16;
+  int64_t need_groups = 2 * c->ncubes + (c->ncubes + 4095) / 4096 + 16;
+  if (ts < need_groups) ts = need_groups;
+  tb.cap_tiles = ts;
+  CK(cudaMalloc(&tb.tile_sum, sizeof(uint32_t) * ts));
+  tb.cap_groups = cap / 1 + c->ncubes + 16;
+  CK(cudaMalloc(&tb.groups, sizeof(uint32_t) * 2 * tb.cap_groups));
+  c->cap = cap;
+  return 0;
+}
+
+// ------------------------------------------------------------------ kernels
+namespace {
+
+__global__ void k_decode_lagrangian(const uint8_t *__restrict__ rec, int64_t np, int64_t stride, int64_t oi,
+                                    int64_t op, int64_t ov, int n, uint32_t *__restrict__ pos,
+                                    float *__restrict__ vel) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint8_t *r = rec + i * stride;
+    uint64_t idx;
+    memcpy(&idx, r + oi, 8);
+    idx = (idx << 8) >> 8;  // PINDX: drop the flag byte (eunha.h:1212)
+    float off[3];
+    memcpy(off, r + op, 12);
+    uint64_t N = (uint64_t)n;
+    uint64_t grid[3] = {idx % N, (idx % (N * N)) / N, idx / (N * N)};
+    for (int a = 0; a < 3; a++) {
+      // XofP: fmod(offset + grid + N, N) (eunha.h:1228-1232), then fixed point
+      double x = fmod((double)off[a] + (double)grid[a] + (double)n, (double)n);
+      double fr = x / (double)n;
+      fr -= floor(fr);
+      double u = rint(fr * 4294967296.0);
+      if (u >= 4294967296.0) u = 0.0;
+      pos[3 * i + a] = (uint32_t)(unsigned long long)u;
+    }
+    if (ov >= 0) {
+      float v[3];
+      memcpy(v, r + ov, 12);
+      vel[3 * i + 0] = v[0];
+      vel[3 * i + 1] = v[1];
+      vel[3 * i + 2] = v[2];
+    } else {
+      vel[3 * i + 0] = vel[3 * i + 1] = vel[3 * i + 2] = 0.f;
+    }
+  }
+}
+
+__global__ void k_store_vel(const float *__restrict__ vel, int64_t np, int64_t stride, int64_t ov,
+                            uint8_t *__restrict__ rec) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    memcpy(rec + i * stride + ov, vel + 3 * i, 12);
+  }
+}
+
+__global__ void k_finish(const uint32_t *__restrict__ perm, int64_t np, const float *__restrict__ fpm,
+                         const float *__restrict__ ftree, unsigned parts, float *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    float f[3] = {0.f, 0.f, 0.f};
+    if (parts & TPM_PART_PM)
+      for (int a = 0; a < 3; a++) f[a] += fpm[3 * i + a];
+    if (parts & TPM_PART_TREE)
+      for (int a = 0; a < 3; a++) f[a] += ftree[3 * i + a];
+    int64_t j = perm[i];
+    out[3 * j + 0] = f[0];
+    out[3 * j + 1] = f[1];
+    out[3 * j + 2] = f[2];
+  }
+}
+
+__global__ void k_kick(const uint32_t *__restrict__ perm, int64_t np, const float *__restrict__ fpm,
+                       const float *__restrict__ ftree, float f2pm, float f2tree, float *__restrict__ vel) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = perm[i];
+    for (int a = 0; a < 3; a++) {
+      float v = vel[3 * j + a];
+      if (f2pm != 0.f) v += f2pm * fpm[3 * i + a];
+      if (f2tree != 0.f) v += f2tree * ftree[3 * i + a];
+      vel[3 * j + a] = v;
+    }
+  }
+}
+
+// x += v * pfact (cells) in FP64, onto the exact periodic fixed point.
+__global__ void k_drift(uint32_t *__restrict__ pos, const float *__restrict__ vel, int64_t np, double pfact,
+                        double units_per_cell) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * np; i += (int64_t)gridDim.x * blockDim.x) {
+    double d = (double)vel[i] * pfact * units_per_cell;
+    double m = fmod(d, 4294967296.0);
+    long long s = llrint(m);
+    pos[i] = pos[i] + (uint32_t)(unsigned long long)s;
+  }
+}
+
+int grid_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 32) b = 148 * 32;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
+  if (!out) return fail(TPM_E_ARG, "out is NULL");
+  *out = nullptr;
+  int rc = check_params(params);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return fail(TPM_E_NODEV, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(TPM_E_ARG, "device %d out of range", device);
+  CK(cudaSetDevice(device));
+  tpm_ctx *c = new tpm_ctx();
+  c->prm = *params;
+  c->device = device;
+  memset(c->stage_ms, 0, sizeof(c->stage_ms));
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(TPM_E_CUDA, "cudaStreamCreate failed");
+  }
+  for (int i = 0; i <= kNStages; i++) cudaEventCreate(&c->ev[i]);
+  if (cudaMalloc(&c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
+      cudaMalloc(&c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
+      cudaMalloc(&c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess) {
+    tpm_destroy(c);
+    return fail(TPM_E_NOMEM, "cudaMalloc of context scratch failed");
+  }
+  c->tb.stack_words = walk_stack_words();
+  if (cudaMalloc(&c->tb.stack, sizeof(uint32_t) * c->tb.stack_words) != cudaSuccess) {
+    tpm_destroy(c);
+    return fail(TPM_E_NOMEM, "cudaMalloc of walk stacks failed");
+  }
+  cudaMemset(c->err, 0, sizeof(uint32_t) * 8);
+  rc = alloc_mesh(c);
+  if (!rc) rc = build_law(c);
+  if (rc) {
+    std::string m = g_err;
+    tpm_destroy(c);
+    return fail(rc, "%s", m.c_str());
+  }
+  *out = c;
+  return 0;
+}
+
+int tpm_destroy(tpm_ctx *c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  free_particles(c);
+  free_mesh(c);
+  if (c->law.t01) cudaFree(c->law.t01);
+  if (c->law.t2) cudaFree(c->law.t2);
+  if (c->err) cudaFree(c->err);
+  if (c->tb.counters) cudaFree(c->tb.counters);
+  if (c->tb.level_range) cudaFree(c->tb.level_range);
+  if (c->tb.stack) cudaFree(c->tb.stack);
+  if (c->stage) cudaFree(c->stage);
+  for (int i = 0; i <= kNStages; i++)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return 0;
+}
+
+int tpm_set_params(tpm_ctx *c, const tpm_params *p) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  int rc = check_params(p);
+  if (rc) return rc;
+  CK(cudaSetDevice(c->device));
+  bool remesh = p->n_mesh != c->prm.n_mesh;
+  c->prm = *p;
+  if (remesh) {
+    CK(cudaStreamSynchronize(c->st));
+    free_particles(c);
+    c->np = 0;
+    rc = alloc_mesh(c);
+    if (rc) return rc;
+  }
+  c->parts_valid = 0;
+  return build_law(c);
+}
+
+int tpm_get_params(const tpm_ctx *c, tpm_params *out) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  *out = c->prm;
+  return 0;
+}
+
+void *tpm_stream(tpm_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+static cudaMemcpyKind kind_in(int mem) { return mem == TPM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; }
+static cudaMemcpyKind kind_out(int mem) { return mem == TPM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost; }
+
+int tpm_load_fixed(tpm_ctx *c, int64_t np, const uint32_t *pos, const float *vel, int mem) {
+  if (!c || !pos || np <= 0) return fail(TPM_E_ARG, "bad arguments to tpm_load_fixed");
+  if (np > 0xffffffffll - 64) return fail(TPM_E_ARG, "np %lld too large", (long long)np);
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_particles(c, np);
+  if (rc) return rc;
+  c->np = np;
+  CK(cudaMemcpyAsync(c->pos, pos, sizeof(uint32_t) * 3 * np, kind_in(mem), c->st));
+  if (vel)
+    CK(cudaMemcpyAsync(c->vel, vel, sizeof(float) * 3 * np, kind_in(mem), c->st));
+  else
+    CK(cudaMemsetAsync(c->vel, 0, sizeof(float) * 3 * np, c->st));
+  c->parts_valid = 0;
+  return 0;
+}
+
+static int ensure_stage(tpm_ctx *c, size_t bytes) {
+  if (bytes <= c->stage_bytes) return 0;
+  if (c->stage) cudaFree(c->stage);
+  c->stage = nullptr;
+  c->stage_bytes = 0;
+  CK(cudaMalloc(&c->stage, bytes));
+  c->stage_bytes = bytes;
+  return 0;
+}
+
+int tpm_load_lagrangian(tpm_ctx *c, int64_t np, const void *particles, int64_t stride, int64_t off_indx,
+                        int64_t off_pos, int64_t off_vel, int mem) {
+  if (!c || !particles || np <= 0 || stride < 20 || off_indx < 0 || off_pos < 0 || off_indx + 8 > stride ||
+      off_pos + 12 > stride || (off_vel >= 0 && off_vel + 12 > stride))
+    return fail(TPM_E_ARG, "bad arguments to tpm_load_lagrangian");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_particles(c, np);
+  if (rc) return rc;
+  c->np = np;
+  const uint8_t *src = (const uint8_t *)particles;
+  if (mem != TPM_MEM_DEVICE) {
+    rc = ensure_stage(c, (size_t)np * stride);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->stage, particles, (size_t)np * stride, cudaMemcpyHostToDevice, c->st));
+    src = (const uint8_t *)c->stage;
+  }
+  k_decode_lagrangian<<<grid_for(np), 256, 0, c->st>>>(src, np, stride, off_indx, off_pos, off_vel,
+                                                       c->prm.n_mesh, c->pos, c->vel);
+  CK(cudaGetLastError());
+  c->parts_valid = 0;
+  return 0;
+}
+
+int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  if ((parts & TPM_PART_ALL) == 0) return fail(TPM_E_ARG, "no force part requested");
+  CK(cudaSetDevice(c->device));
+  const MeshGeom &g = c->g;
+  cudaStream_t st = c->st;
+  int64_t np = c->np;
+  c->launches = 0;
+  CK(cudaMemsetAsync(c->err, 0, sizeof(uint32_t) * 8, st));
+  CK(cudaEventRecord(c->ev[0], st));
+  // ---- sort
+  launch_make_keys(c->pos, np, (uint32_t)g.n, g.sub_bits, c->key, c->val, st);
+  uint64_t *k = c->key;
+  uint32_t *v = c->val;
+  uint64_t *kalt = c->key_alt;
+  uint32_t *valt = c->val_alt;
+  radix_sort_pairs(&k, &v, kalt, valt, np, kKeyBits, c->ss, st, &c->launches);
+  c->skey = k;
+  c->perm = v;
+  launch_gather_pos(c->pos, c->perm, np, c->spos, st);
+  c->launches += 2;
+  CK(cudaEventRecord(c->ev[1], st));
+  // ---- PM
+  if (parts & TPM_PART_PM) {
+    uint32_t ntiles = 1u << (3 * (g.cbits - 3));
+    launch_range_table(c->skey, np, 3 * (g.sub_bits + 3), ntiles, c->tile_start, st);
+    CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
+    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st);
+    c->launches += 2;
+    CK(cudaEventRecord(c->ev[2], st));
+    launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st, &c->launches);
+    CK(cudaEventRecord(c->ev[3], st));
+    launch_fda4(g, &c->tmap, c->phi, c->spos, c->tile_start, c->fpm, c->err, st);
+    c->launches += 1;
+    CK(cudaEventRecord(c->ev[4], st));
+  } else {
+    for (int i = 2; i <= 4; i++) CK(cudaEventRecord(c->ev[i], st));
+  }
+  // ---- tree
+  if (parts & TPM_PART_TREE) {
+    TreeParams tp;
+    tp.n = (uint32_t)g.n;
+    tp.sub_bits = g.sub_bits;
+    tp.theta2 = c->prm.theta * c->prm.theta;
+    tp.rsphere = c->prm.rsphere;
+    tp.cell_per_unit = (float)((double)g.n / 4294967296.0);
+    tp.mass = c->prm.particle_mass;
+    tree_build(tp, c->skey, c->spos, np, c->tb, c->err, st, &c->launches);
+    CK(cudaMemsetAsync(c->tb.counters, 0, sizeof(uint32_t) * 16, st));
+    tree_groups(tp, c->skey, np, c->tb, c->cube_start, c->ncubes, 3 * (g.sub_bits + 2), st, &c->launches);
+    CK(cudaEventRecord(c->ev[5], st));
+    tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
+    CK(cudaEventRecord(c->ev[6], st));
+  } else {
+    for (int i = 5; i <= 6; i++) CK(cudaEventRecord(c->ev[i], st));
+  }
+  CK(cudaEventRecord(c->ev[7], st));
+  CK(cudaGetLastError());
+  uint32_t herr[8];
+  CK(cudaMemcpyAsync(herr, c->err, sizeof(herr), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (herr[0]) {
+    c->parts_valid = 0;
+    if (herr[0] & kErrNodeOverflow) return fail(TPM_E_OVERFLOW, "tree node capacity exceeded");
+    if (herr[0] & kErrStackOverflow) return fail(TPM_E_OVERFLOW, "tree-walk stack overflow");
+    if (herr[0] & kErrTmaTimeout) return fail(TPM_E_CUDA, "TMA load timed out in fda4");
+    return fail(TPM_E_CUDA, "device error flags 0x%x", herr[0]);
+  }
+  for (int s = 0; s < kNStages; s++) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[s], c->ev[s + 1]);
+    c->stage_ms[s] = ms;
+  }
+  // counters: nodes, pp, pc, groups
+  {
+    uint32_t hc[6];
+    uint32_t lr[2 * (kAxisBits + 2)];
+    cudaMemcpy(hc, c->tb.counters, sizeof(hc), cudaMemcpyDeviceToHost);
+    cudaMemcpy(lr, c->tb.level_range, sizeof(lr), cudaMemcpyDeviceToHost);
+    uint32_t nn = 0;
+    for (int l = 0; l <= kAxisBits; l++)
+      if (lr[2 * l + 1] > nn) nn = lr[2 * l + 1];
+    c->counters[0] = (parts & TPM_PART_TREE) ? nn : 0;
+    c->counters[1] = (int64_t)(((uint64_t)hc[3] << 32) | hc[2]);
+    c->counters[2] = (int64_t)(((uint64_t)hc[5] << 32) | hc[4]);
+    c->counters[3] = hc[0];
+  }
+  c->parts_valid = parts & TPM_PART_ALL;
+  return 0;
+}
+
+int tpm_read_forces(tpm_ctx *c, float *out, int mem) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  if (!c->parts_valid) return fail(TPM_E_STATE, "no forces computed");
+  CK(cudaSetDevice(c->device));
+  k_finish<<<grid_for(c->np), 256, 0, c->st>>>(c->perm, c->np, c->fpm, c->ftree, c->parts_valid, c->fout);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->fout, sizeof(float) * 3 * c->np, kind_out(mem), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int tpm_kick(tpm_ctx *c, float fact2_pm, float fact2_tree) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (!c->parts_valid) return fail(TPM_E_STATE, "no forces computed");
+  if (!(c->parts_valid & TPM_PART_PM)) fact2_pm = 0.f;
+  if (!(c->parts_valid & TPM_PART_TREE)) fact2_tree = 0.f;
+  CK(cudaSetDevice(c->device));
+  k_kick<<<grid_for(c->np), 256, 0, c->st>>>(c->perm, c->np, c->fpm, c->ftree, fact2_pm, fact2_tree, c->vel);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int tpm_drift(tpm_ctx *c, double pfact) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  CK(cudaSetDevice(c->device));
+  double upc = 4294967296.0 / (double)c->prm.n_mesh;
+  k_drift<<<grid_for(3 * c->np), 256, 0, c->st>>>(c->pos, c->vel, c->np, pfact, upc);
+  CK(cudaGetLastError());
+  c->parts_valid = 0;
+  return 0;
+}
+
+int tpm_read_velocities(tpm_ctx *c, float *out, int mem) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(out, c->vel, sizeof(float) * 3 * c->np, kind_out(mem), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int tpm_read_positions(tpm_ctx *c, uint32_t *out, int mem) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(out, c->pos, sizeof(uint32_t) * 3 * c->np, kind_out(mem), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+static int store_velocities(tpm_ctx *c, void *particles, int64_t stride, int64_t off_vel, int mem,
+                            bool stage_holds_records) {
+  if (!c || !particles || off_vel < 0 || off_vel + 12 > stride) return fail(TPM_E_ARG, "bad arguments");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  CK(cudaSetDevice(c->device));
+  int64_t np = c->np;
+  if (mem == TPM_MEM_DEVICE) {
+    k_store_vel<<<grid_for(np), 256, 0, c->st>>>(c->vel, np, stride, off_vel, (uint8_t *)particles);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  // the velocities go into a device copy of the record array, which then
+  // replaces the caller's records: fields other than vx,vy,vz keep the
+  // values of that copy
+  int rc = ensure_stage(c, (size_t)np * stride);
+  if (rc) return rc;
+  if (!stage_holds_records)
+    CK(cudaMemcpyAsync(c->stage, particles, (size_t)np * stride, cudaMemcpyHostToDevice, c->st));
+  k_store_vel<<<grid_for(np), 256, 0, c->st>>>(c->vel, np, stride, off_vel, (uint8_t *)c->stage);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(particles, c->stage, (size_t)np * stride, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int tpm_store_lagrangian_velocities(tpm_ctx *c, void *particles, int64_t stride, int64_t off_vel, int mem) {
+  return store_velocities(c, particles, stride, off_vel, mem, false);
+}
+
+int tpm_sync(tpm_ctx *c) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// ---- drop-in forms
+int tpm_pmmain(tpm_ctx *c, void *dm, int64_t np, float fact2) {
+  int rc = tpm_load_lagrangian(c, np, dm, 32, 0, 8, 20, TPM_MEM_HOST);
+  if (!rc) rc = tpm_compute_forces(c, TPM_PART_PM);
+  if (!rc) rc = tpm_kick(c, fact2, 0.f);
+  if (!rc) rc = store_velocities(c, dm, 32, 20, TPM_MEM_HOST, true);
+  return rc;
+}
+
+int tpm_treecorrection(tpm_ctx *c, void *tdm, int64_t np, float fact2) {
+  int rc = tpm_load_lagrangian(c, np, tdm, 40, 8, 16, 28, TPM_MEM_HOST);
+  if (!rc) rc = tpm_compute_forces(c, TPM_PART_TREE);
+  if (!rc) rc = tpm_kick(c, 0.f, fact2);
+  if (!rc) rc = store_velocities(c, tdm, 40, 28, TPM_MEM_HOST, true);
+  return rc;
+}
+
+int tpm_treemain(tpm_ctx *c, void *tdm, int64_t np, float fact2, int stepcount) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  tpm_params p = c->prm;
+  // Treemain.c:598-601
+  p.theta = stepcount < 10 ? 0.3f : (stepcount < 20 ? 0.35f : (stepcount < 60 ? 0.4f : 0.45f));
+  int rc = tpm_set_params(c, &p);
+  if (!rc) rc = tpm_treecorrection(c, tdm, np, fact2);
+  return rc;
+}
+
+int tpm_ewald(tpm_ctx *c, int64_t nt, const int64_t *targets, double *out) {
+  if (!c || !targets || !out || nt <= 0) return fail(TPM_E_ARG, "bad arguments to tpm_ewald");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  for (int64_t i = 0; i < nt; i++)
+    if (targets[i] < 0 || targets[i] >= c->np) return fail(TPM_E_ARG, "target index out of range");
+  CK(cudaSetDevice(c->device));
+  int rc = ewald_force(c->pos, c->np, c->prm.n_mesh, c->prm.epsilon, nt, targets, out, c->st);
+  if (rc) return fail(TPM_E_CUDA, "Ewald kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return 0;
+}
+
+int tpm_stage_times(tpm_ctx *c, float *ms, int n) {
+  if (!c || !ms) return fail(TPM_E_ARG, "NULL argument");
+  int k = n < kNStages ? n : kNStages;
+  for (int i = 0; i < k; i++) ms[i] = c->stage_ms[i];
+  return k;
+}
+
+int tpm_counters(tpm_ctx *c, int64_t *out, int n) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  int k = n < 4 ? n : 4;
+  for (int i = 0; i < k; i++) out[i] = c->counters[i];
+  return k;
+}
+
+int64_t tpm_launch_count(tpm_ctx *c) { return c ? c->launches : 0; }
+
+int tpm_read_order(tpm_ctx *c, uint64_t *keys, uint32_t *perm) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (!c->parts_valid || !c->perm) return fail(TPM_E_STATE, "no forces computed");
+  CK(cudaSetDevice(c->device));
+  if (keys) CK(cudaMemcpyAsync(keys, c->skey, sizeof(uint64_t) * c->np, cudaMemcpyDeviceToHost, c->st));
+  if (perm) CK(cudaMemcpyAsync(perm, c->perm, sizeof(uint32_t) * c->np, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int tpm_read_mesh(tpm_ctx *c, int which, float *out) {
+  if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
+  if (!(c->parts_valid & TPM_PART_PM)) return fail(TPM_E_STATE, "no PM evaluation");
+  CK(cudaSetDevice(c->device));
+  const MeshGeom &g = c->g;
+  int64_t n = g.n;
+  if (which == TPM_MESH_DENSITY) {
+    CK(cudaMemcpyAsync(out, c->rho, sizeof(float) * n * n * n, cudaMemcpyDeviceToHost, c->st));
+  } else if (which == TPM_MESH_POTENTIAL) {
+    // interior of the ghosted potential: n rows of n per z plane at offset kGhost
+    for (int64_t z = 0; z < n; z++)
+      CK(cudaMemcpy2DAsync(out + z * n * n, sizeof(float) * n,
+                           c->phi + kGhost + (int64_t)g.px * (kGhost + (int64_t)g.py * (kGhost + z)),
+                           sizeof(float) * g.px, sizeof(float) * n, n, cudaMemcpyDeviceToHost, c->st));
+  } else {
+    return fail(TPM_E_ARG, "unknown mesh %d", which);
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Internal interfaces between the engine's CUDA translation units.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace tpm {
+
+// ---------------------------------------------------------------- errors
+// Device-side error flags (bit mask) written by kernels with bounded waits
+// or bounded work queues; read by the host after a stage.
+enum DeviceError : uint32_t {
+  kErrStackOverflow = 1u,    // tree-walk node stack full
+  kErrNodeOverflow = 2u,     // tree node capacity exceeded
+  kErrTmaTimeout = 4u,       // a TMA transaction did not complete in time
+  kErrListOverflow = 8u,     // interaction list overflow
+};
+
+// ---------------------------------------------------------------- sort
+struct SortScratch {
+  uint32_t *hist = nullptr;  // [256][ntiles]
+  uint32_t *dtotal = nullptr;  // [256]
+  int64_t cap_tiles = 0;
+};
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+
+void launch_make_keys(const uint32_t *pos, int64_t np, uint32_t n, int sub_bits, uint64_t *key,
+                      uint32_t *val, cudaStream_t st);
+// Stable LSD radix sort of (key, val) pairs on bits [0, nbits). On return
+// *key/*val point at whichever buffer holds the sorted result.
+void radix_sort_pairs(uint64_t **key, uint32_t **val, uint64_t *key_alt, uint32_t *val_alt,
+                      int64_t np, int nbits, SortScratch &scr, cudaStream_t st, int64_t *launches);
+int64_t sort_tiles(int64_t np);
+void launch_gather_pos(const uint32_t *pos, const uint32_t *perm, int64_t np, uint32_t *spos,
+                       cudaStream_t st);
+// start[t] = first sorted index whose key >> shift >= t, t in [0, ntable].
+void launch_range_table(const uint64_t *key, int64_t np, int shift, uint32_t ntable, uint32_t *start,
+                        cudaStream_t st);
+
+// ---------------------------------------------------------------- PM
+struct MeshGeom {
+  int n;          // cells per side
+  int cbits;      // ceil(log2 n)
+  int sub_bits;   // kAxisBits - cbits
+  int tiles_axis; // 2^(cbits-3): Morton tiles per side (tile = 8 cells)
+  int hx;         // n/2 + 1
+  int64_t spec_elems;  // n*n*hx complex
+  int px, py, pz; // ghosted potential pitches (x padded to a multiple of 4)
+};
+constexpr int kTile = 8;     // PM tile: 8^3 cells
+constexpr int kGhost = 4;    // ghost layers of the padded potential
+
+MeshGeom make_geom(int n);
+
+void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
+                        float mass, float *rho, cudaStream_t st);
+// FFT pipeline: rho (n^3 real) -> phi_pad (ghosted potential).
+struct FftPlan {
+  float2 *tw = nullptr;   // twiddles exp(-2 pi i k / L) for L = n and L = n/2
+  float2 *tw_half = nullptr;
+  int n = 0;
+};
+void fft_plan_init(FftPlan &p, int n);
+void fft_plan_free(FftPlan &p);
+void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
+                    float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
+                    int64_t *launches);
+// fda4: gradient and TSC interpolation per tile through TMA.
+void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, const float *phi_pad,
+                 const uint32_t *spos, const uint32_t *tile_start, float *fpm, uint32_t *err,
+                 cudaStream_t st);
+int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out);
+
+// ---------------------------------------------------------------- tree
+struct TreeBuffers {
+  int64_t cap_nodes = 0;
+  uint32_t *start = nullptr, *count = nullptr, *child = nullptr, *nchild = nullptr;
+  uint8_t *level = nullptr;
+  uint4 *geo = nullptr;      // center u32 x3, half-size (float bits)
+  float4 *mom0 = nullptr;    // com (u32 bits x3), mass
+  float4 *mom1 = nullptr;    // Qxx Qyy Qzz Qxy
+  float4 *mom2 = nullptr;    // Qxz Qyz trQ open2 (size^2/theta^2)
+  uint32_t *level_range = nullptr;  // [2*(kAxisBits+2)] begin/end per level
+  uint32_t *tile_sum = nullptr;     // scan scratch
+  int64_t cap_tiles = 0;
+  uint32_t *groups = nullptr;       // walk groups: start | (count << 26) packed as 2 words
+  int64_t cap_groups = 0;
+  uint32_t *counters = nullptr;     // [8]: ngroups, next group, pp, pc, ...
+  uint32_t *stack = nullptr;        // per-warp global stacks
+  int64_t stack_words = 0;
+};
+
+struct TreeParams {
+  uint32_t n;
+  int sub_bits;
+  float theta2;
+  float rsphere;
+  float cell_per_unit;  // n / 2^32
+  float mass;
+};
+
+void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos, int64_t np,
+                TreeBuffers &tb, uint32_t *err, cudaStream_t st, int64_t *launches);
+void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
+                 uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
+                 int64_t *launches);
+// Short-range law table: float4 {d0, s0, d1, s1} and float2 {d2, s2} per entry.
+struct LawTable {
+  float4 *t01 = nullptr;
+  float2 *t2 = nullptr;
+  int entries = 0;
+  float delta = 0, inv_delta = 0;
+};
+void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
+               const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st,
+               int64_t *launches);
+
+// ---------------------------------------------------------------- misc
+void launch_finish_forces(const uint32_t *perm, int64_t np, const float *fpm, const float *ftree,
+                          unsigned parts, float *force_out, cudaStream_t st);
+
+}  // namespace tpm

@@ -1,0 +1,791 @@
+// Particle-mesh long-range force (sm_100a): TSC deposit, a shared-memory
+// pencil FFT with the Green's function fused between the forward and the
+// inverse z transform, and the 4-point gradient + TSC interpolation staged
+// through TMA.
+//
+// Reference path (kjhan0606/LagEunha, GOTPM build):
+//   TSC scatter            Cosmos/pmmain.h:81-159, pmmain.c:112-185
+//   fold into FFT slab     Cosmos/pmmain.c:283-336, RkS/gmigrate.c:212-273
+//   r2c / c2r              Cosmos/pmmain.c:475,492 (FFTW-MPI, unnormalised)
+//   Green's function       Cosmos/psolver.c:13-86
+//   ghosted potential      Cosmos/pmmain.c:337-388
+//   gradient + interp.     Cosmos/fda4.h:11-103,276-384, fda4.c:45-46
+#include <math.h>
+#include <stdio.h>
+
+#include "engine_internal.cuh"
+
+namespace tpm {
+
+MeshGeom make_geom(int n) {
+  MeshGeom g;
+  g.n = n;
+  int c = 0;
+  while ((1 << c) < n) c++;
+  if (c < 3) c = 3;
+  g.cbits = c;
+  g.sub_bits = kAxisBits - c;
+  g.tiles_axis = 1 << (c - 3);
+  g.hx = n / 2 + 1;
+  g.spec_elems = (int64_t)n * n * g.hx;
+  g.px = ((n + 2 * kGhost) + 3) / 4 * 4;
+  g.py = n + 2 * kGhost;
+  g.pz = n + 2 * kGhost;
+  return g;
+}
+
+// ------------------------------------------------------------------ TSC
+// Home node and the three per-axis TSC weights on offsets {-1, 0, +1}
+// relative to it. The reference picks near = rint(x), xmin = x - near,
+// sign = signbit(xmin) ? -1 : 1 and weights w1 = 0.75 - d^2 at near,
+// w2 = 0.5 (0.5 + d)^2 at near + sign, w3 = 0.5 (0.5 - d)^2 at near - sign
+// with d = |xmin| (pmmain.h:86-120). Here w[0], w[1], w[2] are the weights
+// at near-1, near, near+1.
+struct Axis {
+  int near;     // nearest grid node (cells, absolute)
+  float xmin;   // x - near in [-0.5, 0.5]
+};
+
+TPM_D Axis axis_of(uint32_t u, uint32_t n) {
+  uint64_t p = (uint64_t)u * (uint64_t)n;
+  int c = (int)(p >> 32);
+  uint32_t fr = (uint32_t)p;
+  Axis a;
+  if (fr > 0x80000000u) {
+    a.near = c + 1;
+    a.xmin = (float)((double)fr * (1.0 / 4294967296.0) - 1.0);
+  } else {
+    a.near = c;
+    a.xmin = (float)((double)fr * (1.0 / 4294967296.0));
+  }
+  return a;
+}
+
+TPM_D void tsc_w(float xmin, float &w1, float &w2, float &w3, int &sign) {
+  sign = signbit(xmin) ? -1 : 1;
+  float d = fabsf(xmin);
+  w1 = 0.75f - d * d;
+  w3 = 0.5f * (0.25f + d * (d - 1.0f));
+  w2 = w3 + d;
+}
+
+constexpr int kDepNx = 16;            // x extent of the deposit tile: [t-4, t+12)
+constexpr int kDepNy = kTile + 3;     // y/z extent: [t-1, t+9]
+constexpr int kDepCells = kDepNx * kDepNy * kDepNy;
+constexpr int kDepThreads = 256;
+
+__global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
+    const uint32_t *__restrict__ spos, const uint32_t *__restrict__ tile_start, int n, int cbits,
+    float mass, float *__restrict__ rho, int vec4) {
+  __shared__ float acc[kDepCells];
+  int tid = threadIdx.x, lane = tid & 31;
+  // Morton tile index -> tile coordinates
+  uint32_t t = blockIdx.x;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  for (int b = 0; b < cbits - 3; b++) {
+    tx |= ((t >> (3 * b)) & 1u) << b;
+    ty |= ((t >> (3 * b + 1)) & 1u) << b;
+    tz |= ((t >> (3 * b + 2)) & 1u) << b;
+  }
+  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
+  if (p0 == p1) return;
+  int ox = (int)tx * kTile - 4, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
+  for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0.f;
+  __syncthreads();
+  uint32_t nu = (uint32_t)n;
+  int nwarp_items = (int)((p1 - p0 + 31) / 32) * 32;
+  for (int base = 0; base < nwarp_items; base += kDepThreads) {
+    int k = base + tid;
+    bool valid = (uint32_t)k < p1 - p0;
+    // per-axis weights on offsets -1, 0, +1 around the home node
+    float wx[3] = {0, 0, 0}, wy[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+    int hx = 0, hy = 0, hz = 0;
+    if (valid) {
+      int64_t i = (int64_t)p0 + k;
+      Axis ax = axis_of(spos[3 * i + 0], nu), ay = axis_of(spos[3 * i + 1], nu),
+           az = axis_of(spos[3 * i + 2], nu);
+      float w1, w2, w3;
+      int s;
+      tsc_w(ax.xmin, w1, w2, w3, s);
+      wx[1] = w1 * mass;
+      wx[1 + s] = w2 * mass;
+      wx[1 - s] = w3 * mass;
+      tsc_w(ay.xmin, w1, w2, w3, s);
+      wy[1] = w1;
+      wy[1 + s] = w2;
+      wy[1 - s] = w3;
+      tsc_w(az.xmin, w1, w2, w3, s);
+      wz[1] = w1;
+      wz[1 + s] = w2;
+      wz[1 - s] = w3;
+      hx = ax.near - ox;
+      hy = ay.near - oy;
+      hz = az.near - oz;
+    }
+    int home = valid ? hx + kDepNx * (hy + kDepNy * hz) : -1 - lane;
+    int prev = __shfl_up_sync(0xffffffffu, home, 1);
+    bool head = lane == 0 || prev != home;
+    unsigned heads = __ballot_sync(0xffffffffu, head);
+    if (heads == 0xffffffffu) {
+      if (valid) {
+        for (int c = 0; c < 3; c++)
+          for (int b = 0; b < 3; b++)
+            for (int a = 0; a < 3; a++)
+              atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))],
+                        wx[a] * wy[b] * wz[c]);
+      }
+    } else {
+      // runs of equal home node: segmented sum onto the run's first lane
+      unsigned le = heads & ((2u << lane) - 1u);
+      int seg = 31 - __clz(le);
+      bool ok[5];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        int o = 1 << j;
+        int s2 = __shfl_down_sync(0xffffffffu, seg, o);
+        ok[j] = (lane + o < 32) && s2 == seg;
+      }
+      float w[27];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+          for (int a = 0; a < 3; a++) w[a + 3 * b + 9 * c] = wx[a] * wy[b] * wz[c];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+#pragma unroll
+        for (int q = 0; q < 27; q++) {
+          float y = __shfl_down_sync(0xffffffffu, w[q], 1 << j);
+          if (ok[j]) w[q] += y;
+        }
+      }
+      if (valid && head) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+              atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], w[a + 3 * b + 9 * c]);
+      }
+    }
+  }
+  __syncthreads();
+  // flush to the periodic mesh
+  if (vec4) {
+    for (int i = tid; i < kDepCells / 4; i += kDepThreads) {
+      int xq = i % (kDepNx / 4), r = i / (kDepNx / 4);
+      int y = r % kDepNy, z = r / kDepNy;
+      float4 v = *reinterpret_cast<const float4 *>(&acc[4 * xq + kDepNx * (y + kDepNy * z)]);
+      if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+      int gx = ox + 4 * xq, gy = oy + y, gz = oz + z;
+      gx = (gx % n + n) % n;
+      gy = (gy % n + n) % n;
+      gz = (gz % n + n) % n;
+      float4 *dst = reinterpret_cast<float4 *>(rho + gx + (int64_t)n * (gy + (int64_t)n * gz));
+      atomicAdd(dst, v);
+    }
+  } else {
+    for (int i = tid; i < kDepCells; i += kDepThreads) {
+      float v = acc[i];
+      if (v == 0.f) continue;
+      int x = i % kDepNx, r = i / kDepNx;
+      int y = r % kDepNy, z = r / kDepNy;
+      int gx = ((ox + x) % n + n) % n, gy = ((oy + y) % n + n) % n, gz = ((oz + z) % n + n) % n;
+      atomicAdd(rho + gx + (int64_t)n * (gy + (int64_t)n * gz), v);
+    }
+  }
+}
+
+void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
+                        float mass, float *rho, cudaStream_t st) {
+  uint32_t ntiles = 1u << (3 * (g.cbits - 3));
+  int vec4 = (g.n % 4) == 0;
+  k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho, vec4);
+}
+
+// ------------------------------------------------------------------ FFT
+// Stockham autosort radix-4/2/3/5 transform of a batch of pencils held in
+// shared memory (the formulation of Govindaraju et al., SC08): in stage s
+// with radix R and Ns = product of the earlier radices, job j reads
+// in[j + r L/R], twiddles by exp(dir 2 pi i r (j mod Ns) / (Ns R)), does a
+// size-R DFT and writes out[(j / Ns) Ns R + (j mod Ns) + r Ns].
+
+struct Factors {
+  int nf;
+  int r[16];
+};
+
+static Factors factorize(int L) {
+  Factors f;
+  f.nf = 0;
+  while (L % 4 == 0) {
+    f.r[f.nf++] = 4;
+    L /= 4;
+  }
+  while (L % 2 == 0) {
+    f.r[f.nf++] = 2;
+    L /= 2;
+  }
+  while (L % 3 == 0) {
+    f.r[f.nf++] = 3;
+    L /= 3;
+  }
+  while (L % 5 == 0) {
+    f.r[f.nf++] = 5;
+    L /= 5;
+  }
+  if (L != 1) f.nf = -1;
+  return f;
+}
+
+TPM_D float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+TPM_D float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+TPM_D float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+TPM_D float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by dir * i
+TPM_D float2 cmuli(float2 a, float dir) { return make_float2(-dir * a.y, dir * a.x); }
+
+template <int R>
+TPM_D void dft_small(float2 *v, float dir);
+
+template <>
+TPM_D void dft_small<2>(float2 *v, float) {
+  float2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+template <>
+TPM_D void dft_small<4>(float2 *v, float dir) {
+  float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+  float2 s13 = cadd(v[1], v[3]), d13 = cmuli(csub(v[1], v[3]), dir);
+  v[0] = cadd(s02, s13);
+  v[2] = csub(s02, s13);
+  v[1] = cadd(d02, d13);
+  v[3] = csub(d02, d13);
+}
+template <>
+TPM_D void dft_small<3>(float2 *v, float dir) {
+  const float c = -0.5f, s = 0.86602540378443864676f;
+  float2 t = cadd(v[1], v[2]);
+  float2 m = make_float2(v[0].x + c * t.x, v[0].y + c * t.y);
+  float2 d = cmuli(csub(v[1], v[2]), dir * s);
+  v[0] = cadd(v[0], t);
+  v[1] = cadd(m, d);
+  v[2] = csub(m, d);
+}
+template <>
+TPM_D void dft_small<5>(float2 *v, float dir) {
+  const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
+  const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+  float2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+  float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  float2 x0 = v[0];
+  float2 m1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  float2 m2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  // i*dir*(s1 b1 + s2 b2) and i*dir*(s2 b1 - s1 b2)
+  float2 n1 = cmuli(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), dir);
+  float2 n2 = cmuli(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), dir);
+  v[0] = make_float2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+  v[1] = cadd(m1, n1);
+  v[4] = csub(m1, n1);
+  v[2] = cadd(m2, n2);
+  v[3] = csub(m2, n2);
+}
+
+template <int R>
+TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L, int Ns, int P,
+                          float dir, int tid, int nth) {
+  int jobs_per = L / R;
+  int step = L / (Ns * R);
+  for (int job = tid; job < P * jobs_per; job += nth) {
+    int p = job / jobs_per, j = job - p * jobs_per;
+    const float2 *src = in + p * L;
+    float2 *dst = out + p * L;
+    int k = j % Ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      float2 x = src[j + r * jobs_per];
+      if (r) {
+        float2 w = tw[(r * k * step) % L];
+        if (dir > 0) w.y = -w.y;
+        x = cmul(x, w);
+      }
+      v[r] = x;
+    }
+    dft_small<R>(v, dir);
+    int d0 = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) dst[d0 + r * Ns] = v[r];
+  }
+}
+
+// Transforms P pencils of length L from a to scratch b and back as needed;
+// returns the buffer holding the result. dir = -1 forward, +1 backward
+// (unnormalised, FFTW sign convention).
+__device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, int P, float dir,
+                               const int *radix, int nf) {
+  int tid = threadIdx.x, nth = blockDim.x;
+  int Ns = 1;
+  float2 *in = a, *out = b;
+  for (int s = 0; s < nf; s++) {
+    int R = radix[s];
+    if (R == 4)
+      stockham_stage<4>(in, out, tw, L, Ns, P, dir, tid, nth);
+    else if (R == 2)
+      stockham_stage<2>(in, out, tw, L, Ns, P, dir, tid, nth);
+    else if (R == 3)
+      stockham_stage<3>(in, out, tw, L, Ns, P, dir, tid, nth);
+    else
+      stockham_stage<5>(in, out, tw, L, Ns, P, dir, tid, nth);
+    __syncthreads();
+    Ns *= R;
+    float2 *t = in;
+    in = out;
+    out = t;
+  }
+  return in;
+}
+
+struct FftArgs {
+  int n, hx, L;       // mesh size, n/2+1, pencil length of this pass
+  int nf;
+  int radix[16];
+  int P;              // pencils per block
+};
+
+static FftArgs fft_args(int n, int L, int P) {
+  FftArgs a;
+  a.n = n;
+  a.hx = n / 2 + 1;
+  a.L = L;
+  Factors f = factorize(L);
+  a.nf = f.nf;
+  for (int i = 0; i < 16; i++) a.radix[i] = i < f.nf ? f.r[i] : 1;
+  a.P = P;
+  return a;
+}
+
+// twiddle table exp(-2 pi i k / L), k < L
+__global__ void k_twiddles(float2 *tw, int L) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < L) {
+    double s, c;
+    sincospi(-2.0 * (double)k / (double)L, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+}
+
+__global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ spec, struct FftArgs a,
+                            const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n, int64_t nrows);
+__global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__ phi, struct FftArgs a,
+                            const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n, int64_t nrows,
+                            int px, int py);
+__global__ void k_fft_cols(float2 *__restrict__ spec, struct FftArgs a, const float2 *__restrict__ tw_n, int axis,
+                           float dir, int with_green, struct GreenArgs ga, int TX);
+
+void fft_plan_init(FftPlan &p, int n) {
+  p.n = n;
+  const int max_smem = 160 * 1024;
+  cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  cudaMalloc(&p.tw, sizeof(float2) * n);
+  k_twiddles<<<(n + 255) / 256, 256>>>(p.tw, n);
+  int h = n / 2 > 0 ? n / 2 : 1;
+  cudaMalloc(&p.tw_half, sizeof(float2) * h);
+  k_twiddles<<<(h + 255) / 256, 256>>>(p.tw_half, h);
+}
+
+void fft_plan_free(FftPlan &p) {
+  if (p.tw) cudaFree(p.tw);
+  if (p.tw_half) cudaFree(p.tw_half);
+  p.tw = p.tw_half = nullptr;
+}
+
+// r2c along x. Even n: the row is packed as n/2 complex values z_m =
+// x_2m + i x_2m+1, transformed, and split with
+// X_k = (Z_k + conj Z_{L-k})/2 - i/2 W^k (Z_k - conj Z_{L-k}), W = e^{-2 pi i/n}.
+// Odd n: a full complex transform of length n.
+__global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ spec, FftArgs a,
+                            const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n,
+                            int64_t nrows) {
+  extern __shared__ float2 sm[];
+  int L = a.L, P = a.P, n = a.n, hx = a.hx;
+  float2 *twl = sm;
+  float2 *A = sm + L;
+  float2 *B = A + P * L;
+  int tid = threadIdx.x, nth = blockDim.x;
+  for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
+  int64_t row0 = (int64_t)blockIdx.x * P;
+  bool packed = (L * 2 == n);
+  for (int e = tid; e < P * L; e += nth) {
+    int p = e / L, m = e - p * L;
+    int64_t row = row0 + p;
+    float2 v = make_float2(0.f, 0.f);
+    if (row < nrows) {
+      const float *r = rho + row * n;
+      if (packed)
+        v = *reinterpret_cast<const float2 *>(r + 2 * m);
+      else
+        v = make_float2(r[m], 0.f);
+    }
+    A[e] = v;
+  }
+  __syncthreads();
+  float2 *res = fft_pencils(A, B, twl, L, P, -1.f, a.radix, a.nf);
+  for (int e = tid; e < P * hx; e += nth) {
+    int p = e / hx, k = e - p * hx;
+    int64_t row = row0 + p;
+    if (row >= nrows) continue;
+    float2 X;
+    if (packed) {
+      const float2 *Z = res + p * L;
+      float2 zk = Z[k % L], zc = cconj(Z[(L - k) % L]);
+      float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
+      float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));  // times -i below
+      float2 w = tw_n[k % n];
+      float2 wo = cmul(w, make_float2(od.y, -od.x));
+      X = cadd(ev, wo);
+    } else {
+      X = res[p * L + k];
+    }
+    spec[row * hx + k] = X;
+  }
+}
+
+// Complex transform along y (stride hx) or z (stride n*hx) for a block of TX
+// consecutive kx columns. For the z pass with green != 0 the block applies
+// the Green's function between the forward and the inverse transform.
+struct GreenArgs {
+  int law;
+  float sfact;   // reference law: -(pi efold / n)^2
+  float irngc;   // 1 / n^3
+  float rs2k;    // gaussian law: (2 pi rs / n)^2
+  int n;
+};
+
+TPM_D float green(const GreenArgs &g, int kx, int ky, int kz) {
+  float wy = (float)ky, wz = (float)kz;
+  if (wy > g.n / 2.f) wy -= (float)g.n;
+  if (wz > g.n / 2.f) wz -= (float)g.n;
+  float wave = (float)(kx * kx) + wy * wy + wz * wz;
+  if (wave == 0.f) return 0.f;
+  const float fact = -0.31830988618379067154f;  // -1/pi
+  if (g.law == 0) return fact / wave * expf(wave * g.sfact) * g.irngc;
+  // Gaussian split: filter exp(-k^2 rs^2), divided by the squared TSC window
+  // of deposit and interpolation (sinc^3 per axis each).
+  float s = 1.f;
+  int ks[3] = {kx, (int)wy, (int)wz};
+  for (int d = 0; d < 3; d++) {
+    if (ks[d] != 0) {
+      float arg = 3.14159265358979323846f * (float)ks[d] / (float)g.n;
+      float sc = sinf(arg) / arg;
+      float w = sc * sc * sc;
+      s *= w * w;
+    }
+  }
+  return fact / wave * expf(-wave * g.rs2k) * g.irngc / s;
+}
+
+__global__ void k_fft_cols(float2 *__restrict__ spec, FftArgs a, const float2 *__restrict__ tw_n,
+                           int axis, float dir, int with_green, GreenArgs ga, int TX) {
+  extern __shared__ float2 sm[];
+  int n = a.n, hx = a.hx, L = n, P = TX;
+  float2 *twl = sm;
+  float2 *A = sm + L;
+  float2 *B = A + P * L;
+  int tid = threadIdx.x, nth = blockDim.x;
+  for (int k = tid; k < L; k += nth) twl[k] = tw_n[k];
+  int ntx = (hx + TX - 1) / TX;
+  int kx0 = (blockIdx.x % ntx) * TX;
+  int outer = blockIdx.x / ntx;  // z for the y pass, y for the z pass
+  int64_t stride = axis == 1 ? (int64_t)hx : (int64_t)n * hx;
+  int64_t base = axis == 1 ? (int64_t)outer * n * hx : (int64_t)outer * hx;
+  int tw_ = min(TX, hx - kx0);
+  for (int e = tid; e < P * L; e += nth) {
+    int q = e % TX, m = e / TX;  // consecutive threads -> consecutive kx
+    float2 v = make_float2(0.f, 0.f);
+    if (q < tw_) v = spec[base + m * stride + kx0 + q];
+    A[q * L + m] = v;
+  }
+  __syncthreads();
+  float2 *res = fft_pencils(A, B, twl, L, P, dir, a.radix, a.nf);
+  if (with_green) {
+    for (int e = tid; e < P * L; e += nth) {
+      int q = e / L, m = e - q * L;
+      float gk = green(ga, kx0 + q, outer, m);
+      float2 v = res[e];
+      res[e] = make_float2(v.x * gk, v.y * gk);
+    }
+    __syncthreads();
+    float2 *other = res == A ? B : A;
+    res = fft_pencils(res, other, twl, L, P, 1.f, a.radix, a.nf);
+  }
+  for (int e = tid; e < P * L; e += nth) {
+    int q = e % TX, m = e / TX;
+    if (q < tw_) spec[base + m * stride + kx0 + q] = res[q * L + m];
+  }
+}
+
+// c2r along x, written into the ghosted potential phi_pad with kGhost ghost
+// layers on every side (x, y and z ghosts are periodic copies), the layout
+// the fda4 tiles read (Cosmos/pmmain.c:365-382 builds the same ghosts).
+__global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__ phi, FftArgs a,
+                            const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n,
+                            int64_t nrows, int px, int py) {
+  extern __shared__ float2 sm[];
+  int L = a.L, P = a.P, n = a.n, hx = a.hx;
+  float2 *twl = sm;
+  float2 *A = sm + L;
+  float2 *B = A + P * L;
+  int tid = threadIdx.x, nth = blockDim.x;
+  for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
+  int64_t row0 = (int64_t)blockIdx.x * P;
+  bool packed = (L * 2 == n);
+  for (int e = tid; e < P * L; e += nth) {
+    int p = e / L, k = e - p * L;
+    int64_t row = row0 + p;
+    float2 Zk = make_float2(0.f, 0.f);
+    if (row < nrows) {
+      const float2 *X = spec + row * hx;
+      if (packed) {
+        // Z_k = (X_k + conj X_{L-k}) + i conj(W^k) (X_k - conj X_{L-k})
+        float2 xk = X[k], xc = cconj(X[L - k]);
+        if (k == 0) {
+          xk.y = 0.f;
+          xc.y = 0.f;
+        }
+        float2 e2 = cadd(xk, xc), o2 = csub(xk, xc);
+        float2 w = cconj(tw_n[k]);
+        float2 t = cmul(w, o2);
+        Zk = cadd(e2, make_float2(-t.y, t.x));
+      } else {
+        // full Hermitian row for odd n
+        Zk = k < hx ? X[k] : cconj(X[n - k]);
+        if (k == 0) Zk.y = 0.f;
+      }
+    }
+    A[e] = Zk;
+  }
+  __syncthreads();
+  float2 *res = fft_pencils(A, B, twl, L, P, 1.f, a.radix, a.nf);
+  for (int p = 0; p < P; p++) {
+    int64_t row = row0 + p;
+    if (row >= nrows) break;
+    int y = (int)(row % n), z = (int)(row / n);
+    // rows to write: (y, z) and its ghost copies
+    int ys[2] = {y, y < kGhost ? y + n : (y >= n - kGhost ? y - n : 0x7fffffff)};
+    int zs[2] = {z, z < kGhost ? z + n : (z >= n - kGhost ? z - n : 0x7fffffff)};
+    for (int e = tid; e < n + 2 * kGhost; e += nth) {
+      int x = e - kGhost;
+      int xs = (x % n + n) % n;
+      float v;
+      if (packed) {
+        float2 c = res[p * L + (xs >> 1)];
+        v = (xs & 1) ? c.y : c.x;
+      } else {
+        v = res[p * L + xs].x;
+      }
+      for (int iz = 0; iz < 2; iz++) {
+        if (zs[iz] == 0x7fffffff) continue;
+        for (int iy = 0; iy < 2; iy++) {
+          if (ys[iy] == 0x7fffffff) continue;
+          int64_t off = (int64_t)(x + kGhost) + (int64_t)px * ((ys[iy] + kGhost) + (int64_t)py * (zs[iz] + kGhost));
+          phi[off] = v;
+        }
+      }
+    }
+  }
+}
+
+static int pencils_for(int L) {
+  int P = 4096 / L;
+  if (P < 1) P = 1;
+  if (P > 64) P = 64;
+  return P;
+}
+
+void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
+                    float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
+                    int64_t *launches) {
+  int n = g.n;
+  int64_t nrows = (int64_t)n * n;
+  bool packed = (n % 2) == 0;
+  int Lx = packed ? n / 2 : n;
+  int Px = pencils_for(Lx);
+  FftArgs ax = fft_args(n, Lx, Px);
+  const float2 *twL = packed ? p.tw_half : p.tw;
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  int thx = 256;
+  k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho, spec, ax, twL, p.tw, nrows);
+  // columns
+  int TX = n >= 256 ? 8 : 16;
+  if (TX > g.hx) TX = g.hx;
+  FftArgs ac = fft_args(n, n, TX);
+  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  int ntx = (g.hx + TX - 1) / TX;
+  GreenArgs ga;
+  ga.law = law;
+  ga.n = n;
+  ga.sfact = (float)(-pow(M_PI * (double)efold / (double)n, 2));
+  ga.irngc = (float)(1.0 / ((double)n * n * n));
+  ga.rs2k = (float)pow(2.0 * M_PI * (double)rs_split / (double)n, 2);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 1, -1.f, 0, ga, TX);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 2, -1.f, 1, ga, TX);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 1, 1.f, 0, ga, TX);
+  k_fft_x_c2r<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(spec, phi_pad, ax, twL, p.tw, nrows,
+                                                                     g.px, g.py);
+  if (launches) *launches += 5;
+}
+
+// ------------------------------------------------------------------ fda4
+constexpr int kBoxX = 16, kBoxY = kTile + 7, kBoxZ = kTile + 7;  // phi tile + halo
+constexpr int kNodes = kTile + 3;                                 // gradient nodes per axis
+constexpr int kFdaThreads = 256;
+
+TPM_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait on an mbarrier phase; returns false if it did not complete.
+TPM_D bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int64_t limit) {
+  uint32_t addr = smem_u32(bar);
+  for (int64_t it = 0; it < limit; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CUtensorMap tmap,
+                                                      const uint32_t *__restrict__ spos,
+                                                      const uint32_t *__restrict__ tile_start, int n,
+                                                      int cbits, float *__restrict__ fpm,
+                                                      uint32_t *__restrict__ err) {
+  __shared__ __align__(128) float box[kBoxZ][kBoxY][kBoxX];
+  __shared__ float gx[kNodes * kNodes * kNodes], gy[kNodes * kNodes * kNodes],
+      gz[kNodes * kNodes * kNodes];
+  __shared__ __align__(8) uint64_t bar;
+  int tid = threadIdx.x;
+  uint32_t t = blockIdx.x;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  for (int b = 0; b < cbits - 3; b++) {
+    tx |= ((t >> (3 * b)) & 1u) << b;
+    ty |= ((t >> (3 * b + 1)) & 1u) << b;
+    tz |= ((t >> (3 * b + 2)) & 1u) << b;
+  }
+  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
+  if (p0 == p1) return;
+  int x0 = (int)tx * kTile, y0 = (int)ty * kTile, z0 = (int)tz * kTile;
+  if (tid == 0) {
+    uint32_t a = smem_u32(&bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t a = smem_u32(&bar);
+    uint32_t bytes = sizeof(box);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+    // box origin in padded coordinates: x from x0-4 (aligned), y,z from -3
+    int cx = x0 - 4 + kGhost, cy = y0 - 3 + kGhost, cz = z0 - 3 + kGhost;
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(&box[0][0][0])),
+        "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(a)
+        : "memory");
+  }
+  if (!mbar_wait_bounded(&bar, 0, 1ll << 20)) {
+    if (tid == 0) atomicOr(err, (uint32_t)kErrTmaTimeout);
+    mbar_wait_bounded(&bar, 0, 1ll << 20);  // let an in-flight copy land before exit
+    return;
+  }
+  // gradient at nodes [t-1, t+T+1]^3: -dphi/dx with the 4-point stencil
+  const float ff1 = (4.f / 3.f) / 2.f, ff2 = (-1.f / 3.f) / 4.f;
+  for (int i = tid; i < kNodes * kNodes * kNodes; i += kFdaThreads) {
+    int a = i % kNodes, r = i / kNodes;
+    int b = r % kNodes, c = r / kNodes;
+    // node (x0-1+a, y0-1+b, z0-1+c) -> box (a+3, b+2, c+2)
+    int bx = a + 3, by = b + 2, bz = c + 2;
+    gx[i] = ff1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + ff2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]);
+    gy[i] = ff1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + ff2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]);
+    gz[i] = ff1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + ff2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]);
+  }
+  __syncthreads();
+  uint32_t nu = (uint32_t)n;
+  for (uint32_t k = p0 + tid; k < p1; k += kFdaThreads) {
+    Axis ax = axis_of(spos[3 * (int64_t)k + 0], nu), ay = axis_of(spos[3 * (int64_t)k + 1], nu),
+         az = axis_of(spos[3 * (int64_t)k + 2], nu);
+    float wx1, wx2, wx3, wy1, wy2, wy3, wz1, wz2, wz3;
+    int sx, sy, sz;
+    tsc_w(ax.xmin, wx1, wx2, wx3, sx);
+    tsc_w(ay.xmin, wy1, wy2, wy3, sy);
+    tsc_w(az.xmin, wz1, wz2, wz3, sz);
+    // node indices i1 = near, i2 = near + sign, i3 = near - sign (fda4.h:46-54)
+    int i1 = ax.near - (x0 - 1), j1 = ay.near - (y0 - 1), k1 = az.near - (z0 - 1);
+    int ii[3] = {i1, i1 + sx, i1 - sx}, jj[3] = {j1, j1 + sy, j1 - sy}, kk[3] = {k1, k1 + sz, k1 - sz};
+    float wxs[3] = {wx1, wx2, wx3}, wys[3] = {wy1, wy2, wy3}, wzs[3] = {wz1, wz2, wz3};
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    // wt_n in the reference order n = a + 3b + 9c (fda4.h:67-102,276-292)
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        float wxy0 = wxs[0] * wys[b], wxy1 = wxs[1] * wys[b], wxy2 = wxs[2] * wys[b];
+        float wab[3] = {wxy0, wxy1, wxy2};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+          float wt = wab[a] * wzs[c];
+          int node = ii[a] + kNodes * (jj[b] + kNodes * kk[c]);
+          fx += wt * gx[node];
+          fy += wt * gy[node];
+          fz += wt * gz[node];
+        }
+      }
+    fpm[3 * (int64_t)k + 0] = fx;
+    fpm[3 * (int64_t)k + 1] = fy;
+    fpm[3 * (int64_t)k + 2] = fz;
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !p)
+      return -1;
+    fn = (EncodeTiledFn)p;
+  }
+  cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
+  cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.py * 4};
+  cuuint32_t box[3] = {kBoxX, kBoxY, kBoxZ};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, phi_pad, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -2;
+}
+
+void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, const float *phi_pad,
+                 const uint32_t *spos, const uint32_t *tile_start, float *fpm, uint32_t *err,
+                 cudaStream_t st) {
+  (void)phi_pad;
+  uint32_t ntiles = 1u << (3 * (g.cbits - 3));
+  k_fda4<<<ntiles, kFdaThreads, 0, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+}
+
+}  // namespace tpm

@@ -1,0 +1,784 @@
+// Short-range tree correction (sm_100a).
+//
+// The reference builds, for every chaining-mesh bucket of 4^3 cells, an
+// octree over the particles of the 27 surrounding buckets, split at the
+// centre of mass with sub-octants of fewer than 10 particles left as bare
+// particles (OST/ost.ver2.c:36-196), and walks it once per target with the
+// opening test d^2 < size^2/theta^2 (ost.ver2.c:296-306), monopole +
+// quadrupole node terms and particle terms from a tabulated law, both only
+// inside rsphere (ost.ver2.c:247-293; OST/Model4TreeForce.c:34-46).
+//
+// Here one octree covers the whole periodic box. It is built level by level
+// from the Morton-sorted keys (a node's children are the runs of its next
+// octal key digit), keeps the reference's leaf rule (children with fewer than
+// 10 particles stay bare), and carries the same moments: mass, centre of
+// mass, second moments about it, trQ and size^2/theta^2. A warp walks the
+// tree for a group of up to 32 spatially adjacent targets, opening a node if
+// the test would open it for any target of the group, and evaluates the
+// resulting particle and node lists per target with the reference's law and
+// per-target rsphere cuts. Positions are uint32 fixed point; all relative
+// coordinates are exact minimum-image differences converted to float.
+#include <stdio.h>
+
+#include "engine_internal.cuh"
+
+namespace tpm {
+
+constexpr int kBuildTile = 1024;
+constexpr int kBuildThreads = 256;
+constexpr int kBuildGrid = 148 * 4;
+
+TPM_D float wrapf(uint32_t a, uint32_t b, float cpu) { return (float)(int32_t)(a - b) * cpu; }
+
+// child boundary: first index in [lo, hi) whose digit at `shift` is >= d
+TPM_D uint32_t lower_digit(const uint64_t *key, uint32_t lo, uint32_t hi, int shift, uint32_t d) {
+  while (lo < hi) {
+    uint32_t mid = lo + ((hi - lo) >> 1);
+    uint32_t v = (uint32_t)(key[mid] >> shift) & 7u;
+    if (v < d)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_tree_root(int64_t np, TreeBuffers tb, uint32_t n, int sub_bits) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    tb.start[0] = 0;
+    tb.count[0] = (uint32_t)np;
+    tb.child[0] = 0;
+    tb.nchild[0] = 0;
+    tb.level[0] = 0;
+    // root cube: [0, 2^(13-sub_bits)) cells, centre at half of that
+    double half = (double)(1u << (kAxisBits - 1)) / (double)(1u << sub_bits);
+    double cu = half / (double)n;
+    cu = cu - floor(cu);
+    uint32_t c = (uint32_t)(unsigned long long)llrint(cu * 4294967296.0);
+    tb.geo[0] = make_uint4(c, c, c, __float_as_uint((float)half));
+    for (int l = 0; l < 2 * (kAxisBits + 2); l++) tb.level_range[l] = 0;
+    tb.level_range[0] = 0;
+    tb.level_range[1] = 1;
+  }
+}
+
+// Count the non-empty children of every level-l node that splits.
+__global__ void __launch_bounds__(kBuildThreads) k_tree_count(const uint64_t *__restrict__ key,
+                                                              TreeBuffers tb, int l) {
+  uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
+  uint32_t nn = e - b;
+  uint32_t ntiles = (nn + kBuildTile - 1) / kBuildTile;
+  __shared__ uint32_t red[kBuildThreads / 32];
+  int shift = 3 * (kAxisBits - 1 - l);
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    uint32_t local = 0;
+    for (int r = 0; r < kBuildTile / kBuildThreads; r++) {
+      uint32_t i = t * kBuildTile + r * kBuildThreads + threadIdx.x;
+      if (i < nn) {
+        uint32_t node = b + i;
+        uint32_t s = tb.start[node], c = tb.count[node];
+        uint32_t nch = 0;
+        if (c >= (uint32_t)kLeafMin && l < kAxisBits) {
+          uint32_t lo = s, hi = s + c;
+          uint32_t prev = lo;
+          for (uint32_t d = 1; d <= 8; d++) {
+            uint32_t bnd = d < 8 ? lower_digit(key, prev, hi, shift, d) : hi;
+            if (bnd > prev) nch++;
+            prev = bnd;
+          }
+        }
+        tb.nchild[node] = nch;
+        local += nch;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t s = 0;
+      for (int w = 0; w < kBuildThreads / 32; w++) s += red[w];
+      tb.tile_sum[t] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// Exclusive scan of the tile sums of level l and the extent of level l+1.
+__global__ void __launch_bounds__(1024) k_tree_scan(TreeBuffers tb, int l, uint32_t *err) {
+  uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
+  uint32_t ntiles = (e - b + kBuildTile - 1) / kBuildTile;
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t carry;
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < ntiles; base += 1024) {
+    uint32_t i = base + tid;
+    uint32_t v = i < ntiles ? tb.tile_sum[i] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t s = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      wsum[lane] = s;
+    }
+    __syncthreads();
+    if (i < ntiles) tb.tile_sum[i] = carry + (warp ? wsum[warp - 1] : 0u) + x - v;
+    __syncthreads();
+    if (tid == 0) carry += wsum[31];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    uint64_t end = (uint64_t)e + carry;
+    if (end > (uint64_t)tb.cap_nodes) {
+      atomicOr(err, (uint32_t)kErrNodeOverflow);
+      end = e;  // stop refining
+      // leave the level's nodes as leaves
+    }
+    tb.level_range[2 * (l + 1)] = e;
+    tb.level_range[2 * (l + 1) + 1] = (uint32_t)end;
+  }
+}
+
+// Write the children of level-l nodes.
+__global__ void __launch_bounds__(kBuildThreads) k_tree_write(const uint64_t *__restrict__ key,
+                                                              TreeBuffers tb, int l, uint32_t n,
+                                                              int sub_bits) {
+  uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
+  uint32_t e1 = tb.level_range[2 * (l + 1) + 1];
+  bool overflow = (e1 == e);  // capacity hit: nothing written below this level
+  uint32_t nn = e - b;
+  uint32_t ntiles = (nn + kBuildTile - 1) / kBuildTile;
+  __shared__ uint32_t wsum[kBuildThreads / 32];
+  __shared__ uint32_t carry;
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int shift = 3 * (kAxisBits - 1 - l);
+  int child_level = l + 1;
+  // child cube: side 2^(13-child_level) q units
+  uint32_t cside_q = 1u << (kAxisBits - child_level);
+  float half_cells = (float)((double)cside_q * 0.5 / (double)(1u << sub_bits));
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if (tid == 0) carry = tb.tile_sum[t];
+    __syncthreads();
+    for (int r = 0; r < kBuildTile / kBuildThreads; r++) {
+      uint32_t i = t * kBuildTile + r * kBuildThreads + tid;
+      uint32_t node = b + i;
+      uint32_t nch = (i < nn) ? tb.nchild[node] : 0u;
+      if (overflow && i < nn) {
+        nch = 0;
+        tb.nchild[node] = 0;
+      }
+      uint32_t x = nch;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsum[warp] = x;
+      __syncthreads();
+      uint32_t pre = carry;
+      for (int w = 0; w < warp; w++) pre += wsum[w];
+      pre += x - nch;
+      if (i < nn && nch > 0) {
+        uint32_t first = e + pre;
+        tb.child[node] = first;
+        uint32_t s = tb.start[node], c = tb.count[node];
+        uint32_t hi = s + c, prev = s, slot = first;
+        for (uint32_t d = 1; d <= 8; d++) {
+          uint32_t bnd = d < 8 ? lower_digit(key, prev, hi, shift, d) : hi;
+          if (bnd > prev) {
+            tb.start[slot] = prev;
+            tb.count[slot] = bnd - prev;
+            tb.child[slot] = 0;
+            tb.nchild[slot] = 0;
+            tb.level[slot] = (uint8_t)child_level;
+            // cube of the child from its first key
+            uint64_t k = key[prev];
+            uint32_t q[3] = {0, 0, 0};
+            for (int bit = 0; bit < kAxisBits; bit++) {
+              q[0] |= (uint32_t)((k >> (3 * bit)) & 1u) << bit;
+              q[1] |= (uint32_t)((k >> (3 * bit + 1)) & 1u) << bit;
+              q[2] |= (uint32_t)((k >> (3 * bit + 2)) & 1u) << bit;
+            }
+            uint32_t cu[3];
+            for (int a = 0; a < 3; a++) {
+              uint32_t qc = q[a] & ~(cside_q - 1u);
+              double cells = ((double)qc + 0.5 * (double)cside_q) / (double)(1u << sub_bits);
+              double fr = cells / (double)n;
+              fr -= floor(fr);
+              cu[a] = (uint32_t)(unsigned long long)llrint(fr * 4294967296.0);
+            }
+            tb.geo[slot] = make_uint4(cu[0], cu[1], cu[2], __float_as_uint(half_cells));
+            slot++;
+          }
+          prev = bnd;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t s = 0;
+        for (int w = 0; w < kBuildThreads / 32; w++) s += wsum[w];
+        carry += s;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Moments of level-l nodes: leaves from their particles, inner nodes from
+// their children (parallel-axis theorem). size is max |x - com| for leaves
+// and the bound max_c(|com_c - com| + size_c) for inner nodes.
+__global__ void __launch_bounds__(256) k_tree_moments(const uint32_t *__restrict__ spos, TreeBuffers tb,
+                                                      int l, float cpu, float mass, float inv_theta2) {
+  uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
+  for (uint32_t node = b + blockIdx.x * blockDim.x + threadIdx.x; node < e;
+       node += gridDim.x * blockDim.x) {
+    uint4 geo = tb.geo[node];
+    uint32_t nch = tb.nchild[node];
+    float M = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    float qxx = 0, qyy = 0, qzz = 0, qxy = 0, qxz = 0, qyz = 0, size2 = 0.f;
+    if (nch == 0) {
+      uint32_t s = tb.start[node], c = tb.count[node];
+      float sx = 0, sy = 0, sz = 0;
+      for (uint32_t i = s; i < s + c; i++) {
+        sx += wrapf(spos[3 * (int64_t)i + 0], geo.x, cpu);
+        sy += wrapf(spos[3 * (int64_t)i + 1], geo.y, cpu);
+        sz += wrapf(spos[3 * (int64_t)i + 2], geo.z, cpu);
+      }
+      float inv = 1.f / (float)c;
+      cx = sx * inv;
+      cy = sy * inv;
+      cz = sz * inv;
+      M = mass * (float)c;
+      for (uint32_t i = s; i < s + c; i++) {
+        float dx = wrapf(spos[3 * (int64_t)i + 0], geo.x, cpu) - cx;
+        float dy = wrapf(spos[3 * (int64_t)i + 1], geo.y, cpu) - cy;
+        float dz = wrapf(spos[3 * (int64_t)i + 2], geo.z, cpu) - cz;
+        qxx += mass * dx * dx;
+        qyy += mass * dy * dy;
+        qzz += mass * dz * dz;
+        qxy += mass * dx * dy;
+        qxz += mass * dx * dz;
+        qyz += mass * dy * dz;
+        size2 = fmaxf(size2, dx * dx + dy * dy + dz * dz);
+      }
+    } else {
+      uint32_t c0 = tb.child[node];
+      for (uint32_t j = c0; j < c0 + nch; j++) {
+        float4 m0 = tb.mom0[j];
+        float m = m0.w;
+        float dx = wrapf(__float_as_uint(m0.x), geo.x, cpu);
+        float dy = wrapf(__float_as_uint(m0.y), geo.y, cpu);
+        float dz = wrapf(__float_as_uint(m0.z), geo.z, cpu);
+        M += m;
+        cx += m * dx;
+        cy += m * dy;
+        cz += m * dz;
+      }
+      float inv = 1.f / M;
+      cx *= inv;
+      cy *= inv;
+      cz *= inv;
+      float size = 0.f;
+      for (uint32_t j = c0; j < c0 + nch; j++) {
+        float4 m0 = tb.mom0[j], m1 = tb.mom1[j], m2 = tb.mom2[j];
+        float m = m0.w;
+        float dx = wrapf(__float_as_uint(m0.x), geo.x, cpu) - cx;
+        float dy = wrapf(__float_as_uint(m0.y), geo.y, cpu) - cy;
+        float dz = wrapf(__float_as_uint(m0.z), geo.z, cpu) - cz;
+        qxx += m1.x + m * dx * dx;
+        qyy += m1.y + m * dy * dy;
+        qzz += m1.z + m * dz * dz;
+        qxy += m1.w + m * dx * dy;
+        qxz += m2.x + m * dx * dz;
+        qyz += m2.y + m * dy * dz;
+        // child size from its open2 = size^2/theta^2
+        float cs = sqrtf(m2.w / inv_theta2);
+        size = fmaxf(size, sqrtf(dx * dx + dy * dy + dz * dz) + cs);
+      }
+      size2 = size * size;
+    }
+    uint32_t comx = geo.x + (uint32_t)(int32_t)__float2int_rn(cx / cpu);
+    uint32_t comy = geo.y + (uint32_t)(int32_t)__float2int_rn(cy / cpu);
+    uint32_t comz = geo.z + (uint32_t)(int32_t)__float2int_rn(cz / cpu);
+    tb.mom0[node] = make_float4(__uint_as_float(comx), __uint_as_float(comy), __uint_as_float(comz), M);
+    tb.mom1[node] = make_float4(qxx, qyy, qzz, qxy);
+    tb.mom2[node] = make_float4(qxz, qyz, qxx + qyy + qzz, size2 * inv_theta2);
+  }
+}
+
+void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos, int64_t np,
+                TreeBuffers &tb, uint32_t *err, cudaStream_t st, int64_t *launches) {
+  k_tree_root<<<1, 32, 0, st>>>(np, tb, tp.n, tp.sub_bits);
+  int64_t nl = 1;
+  for (int l = 0; l < kAxisBits; l++) {
+    k_tree_count<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l);
+    k_tree_scan<<<1, 1024, 0, st>>>(tb, l, err);
+    k_tree_write<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l, tp.n, tp.sub_bits);
+    nl += 3;
+  }
+  float inv_theta2 = 1.f / tp.theta2;
+  for (int l = kAxisBits; l >= 0; l--) {
+    k_tree_moments<<<kBuildGrid, 256, 0, st>>>(spos, tb, l, tp.cell_per_unit, tp.mass, inv_theta2);
+    nl++;
+  }
+  if (launches) *launches += nl;
+}
+
+// ------------------------------------------------------------ walk groups
+// Groups never cross a 4-cell cube and hold at most 32 particles.
+__global__ void k_group_counts(const uint32_t *__restrict__ cube_start, int64_t ncubes,
+                               uint32_t *__restrict__ gcount) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncubes;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t cnt = cube_start[c + 1] - cube_start[c];
+    gcount[c] = (cnt + 31) / 32;
+  }
+}
+
+// exclusive scan of n u32 values with one block per 4096 and a single-block
+// pass over the block sums
+__global__ void __launch_bounds__(1024) k_scan_block(const uint32_t *in, uint32_t *out, int64_t n,
+                                                     uint32_t *bsum) {
+  __shared__ uint32_t wsum[32];
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int64_t base = (int64_t)blockIdx.x * 4096;
+  uint32_t v[4], s = 0;
+  for (int j = 0; j < 4; j++) {
+    int64_t i = base + 4 * tid + j;
+    v[j] = i < n ? in[i] : 0u;
+    s += v[j];
+  }
+  uint32_t x = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    wsum[lane] = t;
+  }
+  __syncthreads();
+  uint32_t run = (warp ? wsum[warp - 1] : 0u) + x - s;
+  for (int j = 0; j < 4; j++) {
+    int64_t i = base + 4 * tid + j;
+    if (i < n) out[i] = run;
+    run += v[j];
+  }
+  if (tid == 0) bsum[blockIdx.x] = wsum[31];
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *bsum, int64_t nb, uint32_t *total) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t carry;
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < nb; base += 1024) {
+    int64_t i = base + tid;
+    uint32_t v = i < nb ? bsum[i] : 0u;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t s = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+      }
+      wsum[lane] = s;
+    }
+    __syncthreads();
+    if (i < nb) bsum[i] = carry + (warp ? wsum[warp - 1] : 0u) + x - v;
+    __syncthreads();
+    if (tid == 0) carry += wsum[31];
+    __syncthreads();
+  }
+  if (tid == 0) *total = carry;
+}
+
+__global__ void k_write_groups(const uint32_t *__restrict__ cube_start, int64_t ncubes,
+                               const uint32_t *__restrict__ goff, const uint32_t *__restrict__ bsum,
+                               uint32_t *__restrict__ groups) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncubes;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t s = cube_start[c], e = cube_start[c + 1];
+    uint32_t g = goff[c] + bsum[c / 4096];
+    for (uint32_t p = s; p < e; p += 32, g++) {
+      groups[2 * (int64_t)g] = p;
+      groups[2 * (int64_t)g + 1] = min(32u, e - p);
+    }
+  }
+}
+
+void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
+                 uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
+                 int64_t *launches) {
+  (void)tp;
+  launch_range_table(key, np, cube_shift, (uint32_t)ncubes, cube_start, st);
+  // gcount and offsets live in the tail of the group buffer's scratch
+  uint32_t *gcount = tb.tile_sum;  // sized >= ncubes + blocks by the caller
+  uint32_t *goff = gcount + ncubes;
+  int64_t nb = (ncubes + 4095) / 4096;
+  uint32_t *bsum = goff + ncubes;
+  int blocks = (int)((ncubes + 255) / 256);
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_group_counts<<<blocks, 256, 0, st>>>(cube_start, ncubes, gcount);
+  k_scan_block<<<(unsigned)nb, 1024, 0, st>>>(gcount, goff, ncubes, bsum);
+  k_scan_sums<<<1, 1024, 0, st>>>(bsum, nb, &tb.counters[0]);
+  k_write_groups<<<blocks, 256, 0, st>>>(cube_start, ncubes, goff, bsum, tb.groups);
+  if (launches) *launches += 5;
+}
+
+// ------------------------------------------------------------------ walk
+constexpr int kWalkWarps = 8;
+constexpr int kWalkThreads = kWalkWarps * 32;
+constexpr int kStackCap = 8192;
+constexpr int kListCap = 64;
+
+struct WarpLists {
+  uint32_t pc[kListCap];
+  uint32_t pp[kListCap];
+  float stage[32 * 12];
+};
+
+struct WalkCtx {
+  float tx, ty, tz;       // this lane's target relative to u_ref
+  float ax, ay, az;       // accumulated force
+  bool active;
+  uint32_t rx, ry, rz;    // u_ref
+};
+
+TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
+                   float rs2, float mass, const float4 *__restrict__ t01, float delta,
+                   float inv_delta, unsigned long long &npp) {
+  int lane = threadIdx.x & 31;
+  if (lane < m) {
+    uint32_t idx = wl.pp[lane];
+    wl.stage[3 * lane + 0] = wrapf(spos[3 * (int64_t)idx + 0], w.rx, cpu);
+    wl.stage[3 * lane + 1] = wrapf(spos[3 * (int64_t)idx + 1], w.ry, cpu);
+    wl.stage[3 * lane + 2] = wrapf(spos[3 * (int64_t)idx + 2], w.rz, cpu);
+  }
+  __syncwarp();
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for (int j = 0; j < m; j++) {
+    float dx = w.tx - wl.stage[3 * j + 0];
+    float dy = w.ty - wl.stage[3 * j + 1];
+    float dz = w.tz - wl.stage[3 * j + 2];
+    float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= rs2) {
+      float r = sqrtf(r2);
+      int nt = (int)(r * inv_delta);
+      float t = r - (float)nt * delta;
+      float4 c = t01[nt];
+      float f = (c.x + c.y * t) * mass;
+      ax += dx * f;
+      ay += dy * f;
+      az += dz * f;
+    }
+  }
+  if (w.active) {
+    w.ax += ax;
+    w.ay += ay;
+    w.az += az;
+    npp += (unsigned long long)m;
+  }
+  __syncwarp();
+}
+
+TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, float cpu, float rs2,
+                   const float4 *__restrict__ t01, const float2 *__restrict__ t2, float delta,
+                   float inv_delta, int entries, unsigned long long &npc) {
+  int lane = threadIdx.x & 31;
+  for (int base = 0; base < m_all; base += 32) {
+    int m = min(32, m_all - base);
+    if (lane < m) {
+      uint32_t nd = wl.pc[base + lane];
+      float4 m0 = tb.mom0[nd], m1 = tb.mom1[nd], m2 = tb.mom2[nd];
+      float *s = &wl.stage[12 * lane];
+      s[0] = wrapf(__float_as_uint(m0.x), w.rx, cpu);
+      s[1] = wrapf(__float_as_uint(m0.y), w.ry, cpu);
+      s[2] = wrapf(__float_as_uint(m0.z), w.rz, cpu);
+      s[3] = m0.w;
+      s[4] = m1.x;
+      s[5] = m1.y;
+      s[6] = m1.z;
+      s[7] = m1.w;
+      s[8] = m2.x;
+      s[9] = m2.y;
+      s[10] = m2.z;
+    }
+    __syncwarp();
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int j = 0; j < m; j++) {
+      const float *s = &wl.stage[12 * j];
+      float dx = w.tx - s[0], dy = w.ty - s[1], dz = w.tz - s[2];
+      float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 <= rs2) {
+        float r = sqrtf(r2);
+        int nt = (int)(r * inv_delta);
+        float t = r - (float)nt * delta;
+        nt = min(nt, entries - 1);
+        float4 c = t01[nt];
+        float2 c2 = t2[nt];
+        float f1 = c.x + c.y * t, f2 = c.z + c.w * t, f3 = c2.x + c2.y * t;
+        float Qxx = s[4], Qyy = s[5], Qzz = s[6], Qxy = s[7], Qxz = s[8], Qyz = s[9], trQ = s[10];
+        float q1 = Qxx * dx + Qxy * dy + Qxz * dz;
+        float q2 = Qxy * dx + Qyy * dy + Qyz * dz;
+        float q3 = Qxz * dx + Qyz * dy + Qzz * dz;
+        float qq = Qxx * dx * dx + Qyy * dy * dy + Qzz * dz * dz +
+                   2.f * (Qxy * dx * dy + Qxz * dx * dz + Qyz * dy * dz);
+        float tt = s[3] * f1 + trQ * f2 + qq * f3;
+        float two2 = 2.f * f2;
+        ax += dx * tt + q1 * two2;
+        ay += dy * tt + q2 * two2;
+        az += dz * tt + q3 * two2;
+      }
+    }
+    if (w.active) {
+      w.ax += ax;
+      w.ay += ay;
+      w.az += az;
+      npc += (unsigned long long)m;
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
+    const uint32_t *__restrict__ spos, TreeBuffers tb, const float4 *__restrict__ g01,
+    const float2 *__restrict__ g2, int entries, float delta, float inv_delta, float cpu, float rs2,
+    float mass, float *__restrict__ ftree, uint32_t *__restrict__ err) {
+  extern __shared__ float4 smem4[];
+  float4 *t01 = smem4;
+  float2 *t2 = reinterpret_cast<float2 *>(t01 + entries);
+  WarpLists *lists = reinterpret_cast<WarpLists *>(t2 + entries + (entries & 1));
+  for (int i = threadIdx.x; i < entries; i += kWalkThreads) {
+    t01[i] = g01[i];
+    t2[i] = g2[i];
+  }
+  __syncthreads();
+  int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  WarpLists &wl = lists[wib];
+  int64_t gwarp = (int64_t)blockIdx.x * kWalkWarps + wib;
+  uint32_t *stack = tb.stack + gwarp * kStackCap;
+  uint32_t ngroups = tb.counters[0];
+  unsigned long long npp = 0, npc = 0;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  while (true) {
+    uint32_t g = 0;
+    if (lane == 0) g = atomicAdd(&tb.counters[1], 1u);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    if (g >= ngroups) break;
+    uint32_t gs = tb.groups[2 * (int64_t)g], gc = tb.groups[2 * (int64_t)g + 1];
+    WalkCtx w;
+    w.active = (uint32_t)lane < gc;
+    uint32_t ux = 0, uy = 0, uz = 0;
+    if (w.active) {
+      ux = spos[3 * (int64_t)(gs + lane) + 0];
+      uy = spos[3 * (int64_t)(gs + lane) + 1];
+      uz = spos[3 * (int64_t)(gs + lane) + 2];
+    }
+    w.rx = __shfl_sync(0xffffffffu, ux, 0);
+    w.ry = __shfl_sync(0xffffffffu, uy, 0);
+    w.rz = __shfl_sync(0xffffffffu, uz, 0);
+    w.tx = w.active ? wrapf(ux, w.rx, cpu) : 0.f;
+    w.ty = w.active ? wrapf(uy, w.ry, cpu) : 0.f;
+    w.tz = w.active ? wrapf(uz, w.rz, cpu) : 0.f;
+    w.ax = w.ay = w.az = 0.f;
+    float lox = w.tx, hix = w.tx, loy = w.ty, hiy = w.ty, loz = w.tz, hiz = w.tz;
+    for (int o = 16; o > 0; o >>= 1) {
+      lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
+      hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
+      loy = fminf(loy, __shfl_xor_sync(0xffffffffu, loy, o));
+      hiy = fmaxf(hiy, __shfl_xor_sync(0xffffffffu, hiy, o));
+      loz = fminf(loz, __shfl_xor_sync(0xffffffffu, loz, o));
+      hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
+    }
+    float cx = 0.5f * (lox + hix), cy = 0.5f * (loy + hiy), cz = 0.5f * (loz + hiz);
+    float hx = 0.5f * (hix - lox), hy = 0.5f * (hiy - loy), hz = 0.5f * (hiz - loz);
+    // a little slack against float rounding of the relative coordinates
+    float rs2_prune = rs2 * 1.0001f + 1e-4f;
+    int top = 0, npcl = 0, nppl = 0;
+    if (lane == 0) stack[0] = 0;
+    top = 1;
+    __syncwarp();
+    bool failed = false;
+    while (top > 0) {
+      int take = min(top, 32);
+      uint32_t node = 0;
+      bool has = lane < take;
+      if (has) node = stack[top - take + lane];
+      __syncwarp();
+      top -= take;
+      // classify
+      int kind = 0;  // 0 drop, 1 accept (PC), 2 open (push children), 3 particles (PP)
+      uint32_t c0 = 0, nch = 0, ps = 0, pcnt = 0;
+      if (has) {
+        uint4 geo = tb.geo[node];
+        int lev = tb.level[node];
+        float half = __uint_as_float(geo.w);
+        float dx = fmaxf(fabsf(wrapf(geo.x, w.rx, cpu) - cx) - half - hx, 0.f);
+        float dy = fmaxf(fabsf(wrapf(geo.y, w.ry, cpu) - cy) - half - hy, 0.f);
+        float dz = fmaxf(fabsf(wrapf(geo.z, w.rz, cpu) - cz) - half - hz, 0.f);
+        bool near = lev < 2 || dx * dx + dy * dy + dz * dz <= rs2_prune;
+        if (near) {
+          uint32_t cnt = tb.count[node];
+          nch = tb.nchild[node];
+          if (lev > 0 && cnt < (uint32_t)kLeafMin) {
+            kind = 3;
+            ps = tb.start[node];
+            pcnt = cnt;
+          } else {
+            float4 m0 = tb.mom0[node];
+            float open2 = tb.mom2[node].w;
+            float ex = fmaxf(fabsf(wrapf(__float_as_uint(m0.x), w.rx, cpu) - cx) - hx, 0.f);
+            float ey = fmaxf(fabsf(wrapf(__float_as_uint(m0.y), w.ry, cpu) - cy) - hy, 0.f);
+            float ez = fmaxf(fabsf(wrapf(__float_as_uint(m0.z), w.rz, cpu) - cz) - hz, 0.f);
+            bool open = lev < 2 || ex * ex + ey * ey + ez * ez < open2;
+            if (!open)
+              kind = 1;
+            else if (nch > 0) {
+              kind = 2;
+              c0 = tb.child[node];
+            } else {
+              kind = 3;
+              ps = tb.start[node];
+              pcnt = cnt;
+            }
+          }
+        }
+      }
+      // push children
+      uint32_t push = kind == 2 ? nch : 0u;
+      uint32_t incl = push;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      if (top + (int)total > kStackCap) {
+        failed = true;
+        break;
+      }
+      for (uint32_t j = 0; j < push; j++) stack[top + incl - push + j] = c0 + j;
+      top += (int)total;
+      __syncwarp();
+      // accepted nodes
+      unsigned acc = __ballot_sync(0xffffffffu, kind == 1);
+      if (acc) {
+        int cntv = __popc(acc);
+        if (npcl + cntv > kListCap) {
+          eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
+          npcl = 0;
+        }
+        if (kind == 1) wl.pc[npcl + __popc(acc & lanemask_lt)] = node;
+        npcl += cntv;
+        __syncwarp();
+        if (npcl >= 32) {
+          eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
+          npcl = 0;
+        }
+      }
+      // particle ranges, one lane at a time
+      unsigned pr = __ballot_sync(0xffffffffu, kind == 3);
+      while (pr) {
+        int src = __ffs(pr) - 1;
+        pr &= pr - 1;
+        uint32_t s = __shfl_sync(0xffffffffu, ps, src);
+        uint32_t c = __shfl_sync(0xffffffffu, pcnt, src);
+        while (c > 0) {
+          uint32_t room = (uint32_t)(32 - nppl);
+          uint32_t take2 = min(room, c);
+          if ((uint32_t)lane < take2) wl.pp[nppl + lane] = s + lane;
+          nppl += (int)take2;
+          s += take2;
+          c -= take2;
+          __syncwarp();
+          if (nppl == 32) {
+            eval_pp(wl, nppl, spos, w, cpu, rs2, mass, t01, delta, inv_delta, npp);
+            nppl = 0;
+          }
+        }
+      }
+    }
+    if (failed) {
+      if (lane == 0) atomicOr(err, (uint32_t)kErrStackOverflow);
+      continue;
+    }
+    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
+    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpu, rs2, mass, t01, delta, inv_delta, npp);
+    if (w.active) {
+      int64_t i = (int64_t)gs + lane;
+      ftree[3 * i + 0] = w.ax;
+      ftree[3 * i + 1] = w.ay;
+      ftree[3 * i + 2] = w.az;
+    }
+  }
+  // interaction counters
+  for (int o = 16; o > 0; o >>= 1) {
+    npp += __shfl_down_sync(0xffffffffu, npp, o);
+    npc += __shfl_down_sync(0xffffffffu, npc, o);
+  }
+  if (lane == 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[2]), npp);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[4]), npc);
+  }
+}
+
+static int walk_grid(size_t smem) {
+  static int cached = 0;
+  static size_t cached_smem = 0;
+  if (cached && cached_smem == smem) return cached;
+  cudaFuncSetAttribute(k_tree_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_walk, kWalkThreads, smem);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (per_sm < 1) per_sm = 1;
+  cached = per_sm * sms;
+  cached_smem = smem;
+  return cached;
+}
+
+int64_t walk_stack_words() {
+  // enough for the largest grid the walk can use on this device
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (int64_t)sms * 8 * kWalkWarps * kStackCap;
+}
+
+void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
+               const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st, int64_t *launches) {
+  (void)np;
+  size_t smem = sizeof(float4) * law.entries + sizeof(float2) * (law.entries + (law.entries & 1)) +
+                sizeof(WarpLists) * kWalkWarps;
+  int grid = walk_grid(smem);
+  int64_t max_grid = tb.stack_words / ((int64_t)kWalkWarps * kStackCap);
+  if (grid > max_grid) grid = (int)max_grid;
+  k_tree_walk<<<grid, kWalkThreads, smem, st>>>(spos, tb, law.t01, law.t2, law.entries, law.delta,
+                                                law.inv_delta, tp.cell_per_unit,
+                                                tp.rsphere * tp.rsphere, tp.mass, ftree, err);
+  if (launches) *launches += 1;
+}
+
+}  // namespace tpm

@@ -1,0 +1,307 @@
+"""Python front end of the B200 TreePM force engine (ctypes over the C ABI of
+include/tpm_engine.h, implemented by lageunha_b200/libtpm_engine.so).
+
+The engine replaces the GOTPM force evaluation of kjhan0606/LagEunha:
+``pmmain`` (Cosmos/pmmain.c:390), ``treecorrection``
+(Cosmos/treecorrection.c:225) and ``TreeMain`` (Cosmos/Treemain.c:578). The
+methods of the same names here take the reference's particle records (numpy
+structured arrays with the GOTPM layouts of eunha.h:390-412) and add
+``fact2 * F`` to their velocities, as the reference does.
+
+There is no CPU fallback: constructing an Engine without the built library
+or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtpm_engine.so")
+
+TPM_OK = 0
+TPM_LAW_REFERENCE = 0
+TPM_LAW_GAUSSIAN = 1
+PART_PM, PART_TREE, PART_ALL = 1, 2, 3
+MEM_HOST, MEM_DEVICE = 0, 1
+MESH_DENSITY, MESH_POTENTIAL = 0, 1
+STAGES = ("sort", "deposit", "fft", "fda4", "tree_build", "tree_walk", "finish")
+
+# GOTPM record layouts (eunha.h:390-412 with GOTPM defined): the flag byte is
+# the top byte of the 64-bit index (eunha.h:1176-1212).
+DM_DTYPE = np.dtype([("indx", "<u8"), ("x", "<f4"), ("y", "<f4"), ("z", "<f4"),
+                     ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4")])
+TREEDM_DTYPE = np.dtype([("next", "<u8"), ("indx", "<u8"), ("x", "<f4"), ("y", "<f4"), ("z", "<f4"),
+                         ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4")])
+assert DM_DTYPE.itemsize == 32 and TREEDM_DTYPE.itemsize == 40
+
+
+class TpmParams(ctypes.Structure):
+    _fields_ = [("n_mesh", ctypes.c_int32), ("law", ctypes.c_int32), ("theta", ctypes.c_float),
+                ("rsphere", ctypes.c_float), ("epsilon", ctypes.c_float), ("efold", ctypes.c_float),
+                ("rs_split", ctypes.c_float), ("particle_mass", ctypes.c_float)]
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tpm error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# every function declared in include/tpm_engine.h with its ctypes signature
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_SIGS = {
+    "tpm_default_params": (None, [ctypes.POINTER(TpmParams), ctypes.c_int32]),
+    "tpm_last_error": (ctypes.c_char_p, []),
+    "tpm_version": (ctypes.c_char_p, []),
+    "tpm_create": (ctypes.c_int, [ctypes.POINTER(TpmParams), ctypes.c_int, ctypes.POINTER(_P)]),
+    "tpm_destroy": (ctypes.c_int, [_P]),
+    "tpm_set_params": (ctypes.c_int, [_P, ctypes.POINTER(TpmParams)]),
+    "tpm_get_params": (ctypes.c_int, [_P, ctypes.POINTER(TpmParams)]),
+    "tpm_load_fixed": (ctypes.c_int, [_P, _I64, _P, _P, ctypes.c_int]),
+    "tpm_load_lagrangian": (ctypes.c_int, [_P, _I64, _P, _I64, _I64, _I64, _I64, ctypes.c_int]),
+    "tpm_compute_forces": (ctypes.c_int, [_P, ctypes.c_uint]),
+    "tpm_read_forces": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_kick": (ctypes.c_int, [_P, ctypes.c_float, ctypes.c_float]),
+    "tpm_drift": (ctypes.c_int, [_P, ctypes.c_double]),
+    "tpm_read_velocities": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_read_positions": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_store_lagrangian_velocities": (ctypes.c_int, [_P, _P, _I64, _I64, ctypes.c_int]),
+    "tpm_sync": (ctypes.c_int, [_P]),
+    "tpm_stream": (_P, [_P]),
+    "tpm_pmmain": (ctypes.c_int, [_P, _P, _I64, ctypes.c_float]),
+    "tpm_treecorrection": (ctypes.c_int, [_P, _P, _I64, ctypes.c_float]),
+    "tpm_treemain": (ctypes.c_int, [_P, _P, _I64, ctypes.c_float, ctypes.c_int]),
+    "tpm_ewald": (ctypes.c_int, [_P, _I64, _P, _P]),
+    "tpm_stage_times": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_counters": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_launch_count": (_I64, [_P]),
+    "tpm_read_order": (ctypes.c_int, [_P, _P, _P]),
+    "tpm_read_mesh": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+}
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libtpm_engine.so; raises if it is missing (no silent fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m lageunha_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != TPM_OK:
+        raise EngineError(rc, load_library().tpm_last_error().decode())
+
+
+def _ptr(a):
+    """(pointer, mem) of a numpy array (host) or a CUDA torch tensor (device)."""
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data, MEM_HOST
+    if hasattr(a, "data_ptr") and hasattr(a, "is_cuda"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr(), (MEM_DEVICE if a.is_cuda else MEM_HOST)
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def default_params(n_mesh: int) -> TpmParams:
+    p = TpmParams()
+    load_library().tpm_default_params(ctypes.byref(p), n_mesh)
+    return p
+
+
+class Engine:
+    """One periodic box on one GPU (a tpm_ctx)."""
+
+    def __init__(self, n_mesh: int, *, theta: float = 0.3, rsphere: float = 4.0, epsilon: float = 0.1,
+                 efold: float = 0.9, law: str | int = "reference", rs_split: float = 1.25,
+                 particle_mass: float = 1.0, device: int = 0):
+        lib = load_library()
+        p = default_params(n_mesh)
+        p.theta, p.rsphere, p.epsilon, p.efold = theta, rsphere, epsilon, efold
+        p.law = {"reference": TPM_LAW_REFERENCE, "gaussian": TPM_LAW_GAUSSIAN}.get(law, law)
+        p.rs_split, p.particle_mass = rs_split, particle_mass
+        ctx = ctypes.c_void_p()
+        _check(lib.tpm_create(ctypes.byref(p), device, ctypes.byref(ctx)))
+        self._lib, self._ctx, self.n_mesh, self.np = lib, ctx, n_mesh, 0
+
+    # ---------------------------------------------------------------- lifecycle
+    def close(self):
+        if self._ctx:
+            self._lib.tpm_destroy(self._ctx)
+            self._ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> TpmParams:
+        p = TpmParams()
+        _check(self._lib.tpm_get_params(self._ctx, ctypes.byref(p)))
+        return p
+
+    def set_params(self, **kw):
+        p = self.params
+        for k, v in kw.items():
+            if k == "law":
+                v = {"reference": TPM_LAW_REFERENCE, "gaussian": TPM_LAW_GAUSSIAN}.get(v, v)
+            setattr(p, k, v)
+        _check(self._lib.tpm_set_params(self._ctx, ctypes.byref(p)))
+        self.n_mesh = p.n_mesh
+
+    @property
+    def stream(self) -> int:
+        return self._lib.tpm_stream(self._ctx) or 0
+
+    # ---------------------------------------------------------------- state
+    def load_fixed(self, pos_u32, vel=None):
+        """pos_u32: (np, 3) uint32 fixed point (numpy or CUDA tensor)."""
+        np_ = int(pos_u32.shape[0])
+        pp, mem = _ptr(pos_u32)
+        vp = None
+        if vel is not None:
+            vp, vmem = _ptr(vel)
+            if vmem != mem:
+                raise ValueError("positions and velocities must live in the same memory")
+        _check(self._lib.tpm_load_fixed(self._ctx, np_, pp, vp, mem))
+        self.np = np_
+
+    def load_lagrangian(self, records, off_indx=None, off_pos=None, off_vel=None):
+        """records: structured array with DM_DTYPE or TREEDM_DTYPE fields."""
+        dt = records.dtype
+        oi = dt.fields["indx"][1] if off_indx is None else off_indx
+        op = dt.fields["x"][1] if off_pos is None else off_pos
+        ov = (dt.fields["vx"][1] if "vx" in dt.fields else -1) if off_vel is None else off_vel
+        rp, mem = _ptr(records)
+        _check(self._lib.tpm_load_lagrangian(self._ctx, records.shape[0], rp, dt.itemsize, oi, op, ov, mem))
+        self.np = int(records.shape[0])
+
+    def compute(self, parts: int = PART_ALL):
+        _check(self._lib.tpm_compute_forces(self._ctx, parts))
+
+    def forces(self, out=None):
+        if out is None:
+            out = np.empty((self.np, 3), np.float32)
+        op, mem = _ptr(out)
+        _check(self._lib.tpm_read_forces(self._ctx, op, mem))
+        return out
+
+    def kick(self, fact2_pm: float, fact2_tree: float):
+        _check(self._lib.tpm_kick(self._ctx, fact2_pm, fact2_tree))
+
+    def drift(self, pfact: float):
+        _check(self._lib.tpm_drift(self._ctx, pfact))
+
+    def velocities(self, out=None):
+        if out is None:
+            out = np.empty((self.np, 3), np.float32)
+        op, mem = _ptr(out)
+        _check(self._lib.tpm_read_velocities(self._ctx, op, mem))
+        return out
+
+    def positions(self, out=None):
+        if out is None:
+            out = np.empty((self.np, 3), np.uint32)
+        op, mem = _ptr(out)
+        _check(self._lib.tpm_read_positions(self._ctx, op, mem))
+        return out
+
+    def sync(self):
+        _check(self._lib.tpm_sync(self._ctx))
+
+    # ---------------------------------------------------------------- drop-in
+    def pmmain(self, dm_records: np.ndarray, fact2: float = 1.0):
+        """pmmain (Cosmos/pmmain.c:390) on GOTPM dmparticletype records:
+        v += fact2 * F_PM in place."""
+        if dm_records.dtype != DM_DTYPE:
+            raise TypeError("pmmain wants DM_DTYPE records")
+        _check(self._lib.tpm_pmmain(self._ctx, dm_records.ctypes.data, dm_records.shape[0], fact2))
+        self.np = int(dm_records.shape[0])
+
+    def treecorrection(self, tdm_records: np.ndarray, fact2: float = 1.0):
+        """treecorrection (Cosmos/treecorrection.c:225) on treedmparticletype
+        records: v += fact2 * F_tree in place."""
+        if tdm_records.dtype != TREEDM_DTYPE:
+            raise TypeError("treecorrection wants TREEDM_DTYPE records")
+        _check(self._lib.tpm_treecorrection(self._ctx, tdm_records.ctypes.data, tdm_records.shape[0], fact2))
+        self.np = int(tdm_records.shape[0])
+
+    def treemain(self, tdm_records: np.ndarray, fact2: float, stepcount: int):
+        """TreeMain for GOTPM (Cosmos/Treemain.c:578-664)."""
+        if tdm_records.dtype != TREEDM_DTYPE:
+            raise TypeError("treemain wants TREEDM_DTYPE records")
+        _check(self._lib.tpm_treemain(self._ctx, tdm_records.ctypes.data, tdm_records.shape[0], fact2, stepcount))
+        self.np = int(tdm_records.shape[0])
+
+    # ---------------------------------------------------------------- diagnostics
+    def ewald(self, targets) -> np.ndarray:
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        out = np.empty((t.shape[0], 3), np.float64)
+        _check(self._lib.tpm_ewald(self._ctx, t.shape[0], t.ctypes.data, out.ctypes.data))
+        return out
+
+    def stage_times(self) -> dict:
+        ms = np.zeros(len(STAGES), np.float32)
+        k = self._lib.tpm_stage_times(self._ctx, ms.ctypes.data, len(STAGES))
+        return {STAGES[i]: float(ms[i]) for i in range(k)}
+
+    def counters(self) -> dict:
+        c = np.zeros(4, np.int64)
+        self._lib.tpm_counters(self._ctx, c.ctypes.data, 4)
+        return {"nodes": int(c[0]), "pp": int(c[1]), "pc": int(c[2]), "groups": int(c[3])}
+
+    def launch_count(self) -> int:
+        return int(self._lib.tpm_launch_count(self._ctx))
+
+    def order(self):
+        keys = np.empty(self.np, np.uint64)
+        perm = np.empty(self.np, np.uint32)
+        _check(self._lib.tpm_read_order(self._ctx, keys.ctypes.data, perm.ctypes.data))
+        return keys, perm
+
+    def mesh(self, which: int = MESH_DENSITY) -> np.ndarray:
+        out = np.empty(self.n_mesh ** 3, np.float32)
+        _check(self._lib.tpm_read_mesh(self._ctx, which, out.ctypes.data))
+        return out.reshape(self.n_mesh, self.n_mesh, self.n_mesh)
+
+
+def dm_records(ps) -> np.ndarray:
+    """GOTPM dmparticletype records of a ParticleSet (lageunha_b200.ic)."""
+    r = np.zeros(ps.np, DM_DTYPE)
+    r["indx"] = ps.indx
+    r["x"], r["y"], r["z"] = ps.offset[:, 0], ps.offset[:, 1], ps.offset[:, 2]
+    r["vx"], r["vy"], r["vz"] = ps.vel[:, 0], ps.vel[:, 1], ps.vel[:, 2]
+    return r
+
+
+def treedm_records(ps) -> np.ndarray:
+    r = np.zeros(ps.np, TREEDM_DTYPE)
+    r["indx"] = ps.indx
+    r["x"], r["y"], r["z"] = ps.offset[:, 0], ps.offset[:, 1], ps.offset[:, 2]
+    r["vx"], r["vy"], r["vz"] = ps.vel[:, 0], ps.vel[:, 1], ps.vel[:, 2]
+    return r

@@ -1,0 +1,158 @@
+"""Seeded synthetic particle sets for the TreePM force engine.
+
+Zel'dovich-displaced lattices of a Gaussian random field with a power-law
+spectrum, optionally with Plummer spheres planted in place of field
+particles. The reference builds its initial conditions from CAMB spectra
+(Cosmos/CosmosIC/Zeldovich.c:14-100, Cosmos/CosmosIC/MakeParticle.c:149-212);
+these seeded sets stand in for them with the shapes, sizes and displacement
+statistics the workloads name.
+
+Two position encodings are produced:
+  * the reference's XYZDBL form: a Lagrangian lattice index
+    i + N*(j + N*k) plus a float offset from that lattice point
+    (Cosmos/CosmosIC/cosmosic.h:285-288, eunha.h:1228-1232);
+  * the engine's form: per axis a uint32 fixed-point coordinate
+    u = round(frac(x/N) * 2^32), which wraps exactly with the period.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class ParticleSet:
+    n_mesh: int            # PM mesh cells per side (== lattice size here)
+    box_mpc: float         # box side in Mpc/h (metadata)
+    indx: np.ndarray       # (np,) uint64 Lagrangian index
+    offset: np.ndarray     # (np, 3) float32 displacement from the lattice point, cells
+    vel: np.ndarray        # (np, 3) float32 velocities (code units)
+    seed: int
+
+    @property
+    def np(self) -> int:
+        return int(self.indx.shape[0])
+
+    def positions_f64(self) -> np.ndarray:
+        """Decoded positions in [0, N) cells, as eunha.h:1228-1232 computes them."""
+        return decode_positions(self.n_mesh, self.indx, self.offset)
+
+    def positions_u32(self) -> np.ndarray:
+        """(np, 3) uint32 fixed-point positions (engine layout, AoS)."""
+        return to_fixed_point(self.positions_f64(), self.n_mesh)
+
+
+def decode_positions(n: int, indx: np.ndarray, offset: np.ndarray) -> np.ndarray:
+    idx = (indx.astype(np.uint64) << np.uint64(8)) >> np.uint64(8)
+    nn = np.uint64(n)
+    grid = np.stack([idx % nn, (idx % (nn * nn)) // nn, idx // (nn * nn)], axis=1).astype(np.float64)
+    return np.fmod(offset.astype(np.float64) + grid + n, float(n))
+
+
+def to_fixed_point(pos: np.ndarray, n: int) -> np.ndarray:
+    """round(frac(x/N) * 2^32) mod 2^32, computed in float64."""
+    frac = np.mod(pos / float(n), 1.0)
+    u = np.rint(frac * 4294967296.0)
+    u = np.where(u >= 4294967296.0, 0.0, u)
+    return u.astype(np.uint64).astype(np.uint32)
+
+
+def from_fixed_point(u: np.ndarray, n: int) -> np.ndarray:
+    return u.astype(np.float64) * (float(n) / 4294967296.0)
+
+
+def _displacement_field(n: int, rng: np.random.Generator, spec_index: float, damp: float,
+                        rms_target: float) -> np.ndarray:
+    """Zel'dovich displacement psi = IFFT[i k delta_k / k^2] of a Gaussian
+    field with P(k) = A k^n exp(-(damp k)^2) (k in radians per cell), scaled so
+    that the rms of |psi| equals rms_target cells. Returns (3, n, n, n) [z][y][x]."""
+    white = rng.standard_normal((n, n, n), dtype=np.float64)
+    wk = np.fft.rfftn(white)
+    kz = 2 * np.pi * np.fft.fftfreq(n)[:, None, None]
+    ky = 2 * np.pi * np.fft.fftfreq(n)[None, :, None]
+    kx = 2 * np.pi * np.fft.rfftfreq(n)[None, None, :]
+    k2 = kx * kx + ky * ky + kz * kz
+    k2[0, 0, 0] = 1.0
+    amp = np.power(k2, spec_index / 4.0) * np.exp(-0.5 * damp * damp * k2)
+    amp[0, 0, 0] = 0.0
+    dk = wk * amp
+    psi = np.empty((3, n, n, n), dtype=np.float64)
+    for c, kc in enumerate((kx, ky, kz)):
+        psi[c] = np.fft.irfftn(1j * kc * dk / k2, s=(n, n, n))
+    rms = np.sqrt(np.mean(np.sum(psi * psi, axis=0)))
+    psi *= rms_target / rms
+    return psi
+
+
+def _wrap_offset(off: np.ndarray, n: int) -> np.ndarray:
+    return (off + 0.5 * n) % n - 0.5 * n
+
+
+def zeldovich(n: int, seed: int, spec_index: float = -2.0, damp: float = 0.5,
+              rms_disp: float = 0.3, box_mpc: float = 100.0, vel_factor: float = 0.0) -> ParticleSet:
+    """n^3 particles on an n^3 mesh, displaced from the lattice by psi."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    psi = _displacement_field(n, rng, spec_index, damp, rms_disp)
+    # lattice index i + n*(j + n*k) for the point (x=i, y=j, z=k)
+    offset = np.stack([psi[0].ravel(), psi[1].ravel(), psi[2].ravel()], axis=1)
+    offset = _wrap_offset(offset, n).astype(np.float32)
+    indx = np.arange(n ** 3, dtype=np.uint64)
+    vel = (vel_factor * offset).astype(np.float32)
+    return ParticleSet(n, box_mpc, indx, offset, vel, seed)
+
+
+def plant_plummer(ps: ParticleSet, seed: int, n_spheres: int, scale_cells: float,
+                  nmin: int, nmax: int) -> ParticleSet:
+    """Replace randomly chosen field particles by n_spheres Plummer spheres
+    of scale radius scale_cells, each with a particle count drawn uniformly in
+    [nmin, nmax]; the total particle count does not change."""
+    n = ps.n_mesh
+    rng = np.random.Generator(np.random.PCG64(seed + 7919))
+    counts = rng.integers(nmin, nmax + 1, size=n_spheres)
+    centres = rng.random((n_spheres, 3)) * n
+    total = int(counts.sum())
+    if total > ps.np // 2:
+        raise ValueError("Plummer spheres would replace more than half of the particles")
+    chosen = rng.choice(ps.np, size=total, replace=False)
+    # Plummer radius from the cumulative mass M(<r)/M = r^3/(r^2+a^2)^{3/2}
+    u = rng.random(total) * 0.99
+    r = scale_cells / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    cth = rng.uniform(-1, 1, total)
+    phi = rng.uniform(0, 2 * np.pi, total)
+    sth = np.sqrt(1 - cth * cth)
+    d = np.stack([r * sth * np.cos(phi), r * sth * np.sin(phi), r * cth], axis=1)
+    cid = np.repeat(np.arange(n_spheres), counts)
+    target = np.mod(centres[cid] + d, n)
+    grid = decode_positions(n, ps.indx[chosen], np.zeros((total, 3), np.float32))
+    offset = ps.offset.copy()
+    offset[chosen] = _wrap_offset(target - grid, n).astype(np.float32)
+    vel = ps.vel.copy()
+    vel[chosen] = 0.0
+    return ParticleSet(n, ps.box_mpc, ps.indx.copy(), offset, vel, ps.seed)
+
+
+def workload(name: str, scale: int | None = None) -> ParticleSet:
+    """The named synthetic workloads. `scale` overrides the mesh size (for
+    parity-sized cases with the same statistics).
+
+    plain64:      64^3, L=100 Mpc/h, P(k) = A k^-2 exp(-(0.5 k)^2), rms 0.3
+    clustered256: 256^3, L=200, same P(k) form, rms 1.5, plus 200 Plummer
+                  spheres (a = 0.5 Mpc/h = 0.64 cells, 2000-20000 particles)
+    scale512:     512^3, L=500, P(k) ~ k^-2.5, rms 2, v = 0.5 psi
+    """
+    if name == "plain64":
+        n = scale or 64
+        return zeldovich(n, seed=1, spec_index=-2.0, damp=0.5, rms_disp=0.3, box_mpc=100.0)
+    if name == "clustered256":
+        n = scale or 256
+        ps = zeldovich(n, seed=2, spec_index=-2.0, damp=0.5, rms_disp=1.5, box_mpc=200.0)
+        frac = (n / 256.0) ** 3
+        nsph = max(1, int(round(200 * frac))) if n < 256 else 200
+        a_cells = 0.5 / 200.0 * 256.0
+        return plant_plummer(ps, seed=2, n_spheres=nsph, scale_cells=a_cells, nmin=2000 if n >= 128 else 200,
+                             nmax=20000 if n >= 128 else 2000)
+    if name == "scale512":
+        n = scale or 512
+        return zeldovich(n, seed=3, spec_index=-2.5, damp=0.5, rms_disp=2.0, box_mpc=500.0, vel_factor=0.5)
+    raise KeyError(name)

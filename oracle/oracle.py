@@ -1,0 +1,216 @@
+"""ctypes front end of the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/liboracle.so (the C restatement, tpm_oracle.c) and, where built,
+oracle/_ref/libref_{A,B}.so (the reference's own force-path sources compiled
+with the single-rank harness ref_shim.c). Only tests/, the smoke check and
+bench.py's CPU-baseline leg import this module; the engine never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+VARIANT_A, VARIANT_B = 0, 1
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_flt = ctypes.c_float
+_dbl = ctypes.c_double
+
+_lib = None
+_ref = {}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so is not built (run `make -C oracle oracle`)")
+        L = ctypes.CDLL(path)
+        L.or_decode.argtypes = [_int, _i64, _u64p, _f32p, _f64p]
+        L.or_tsc_density.argtypes = [_int, _i64, _f64p, _f32p]
+        L.or_potential.argtypes = [_int, _i64, _f64p, _flt, _f32p]
+        L.or_pm_force.argtypes = [_int, _i64, _f64p, _flt, _f32p]
+        L.or_fda4_force.argtypes = [_int, _i64, _f64p, _f32p, _f32p]
+        L.or_spline_table.argtypes = [_int, _flt, _f64p, _f64p]
+        L.or_tree_force.argtypes = [_int, _i64, _f64p, _flt, _flt, _flt, _int, _f32p]
+        L.or_direct_short_force.argtypes = [_int, _i64, _f64p, _flt, _flt, _i64, _i64p, _f64p]
+        L.or_ewald_force.argtypes = [_int, _i64, _f64p, _flt, _i64, _i64p, _dbl, _dbl, _int, _f64p]
+        for f in ("or_decode",):
+            getattr(L, f).restype = None
+        _lib = L
+    return _lib
+
+
+def ref_available(variant: int = VARIANT_B) -> bool:
+    return os.path.exists(_ref_path(variant))
+
+
+def _ref_path(variant):
+    return os.path.join(HERE, "_ref", "libref_%s.so" % ("A" if variant == VARIANT_A else "B"))
+
+
+def ref(variant: int = VARIANT_B):
+    if variant not in _ref:
+        path = _ref_path(variant)
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is not built (needs the reference tree; `make -C oracle ref`)")
+        L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        L.ref_pm_force.argtypes = [_int, _i64, _u64p, _f32p, _flt, _f32p]
+        L.ref_tree_force.argtypes = [_int, _i64, _u64p, _f32p, _flt, _flt, _flt, _f32p]
+        L.ref_tsc_density.argtypes = [_int, _i64, _u64p, _f32p, _f32p]
+        L.ref_potential.argtypes = [_int, _i64, _u64p, _f32p, _flt, _f32p]
+        L.ref_spline_table.argtypes = [_int, _flt, _f64p, _f64p]
+        _ref[variant] = L
+    return _ref[variant]
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ---------------------------------------------------------------- restatement
+def decode(n, indx, off):
+    np_ = indx.shape[0]
+    out = np.empty((np_, 3), np.float64)
+    lib().or_decode(n, np_, _c(indx, np.uint64), _c(off, np.float32), out)
+    return out
+
+
+def tsc_density(n, pos):
+    out = np.empty(n ** 3, np.float32)
+    lib().or_tsc_density(n, pos.shape[0], _c(pos, np.float64), out)
+    return out.reshape(n, n, n)
+
+
+def potential(n, pos, efold=0.9):
+    out = np.empty(n ** 3, np.float32)
+    lib().or_potential(n, pos.shape[0], _c(pos, np.float64), efold, out)
+    return out.reshape(n, n, n)
+
+
+def pm_force(n, pos, efold=0.9):
+    out = np.empty((pos.shape[0], 3), np.float32)
+    lib().or_pm_force(n, pos.shape[0], _c(pos, np.float64), efold, out)
+    return out
+
+
+def fda4_force(n, pos, phi):
+    out = np.empty((pos.shape[0], 3), np.float32)
+    lib().or_fda4_force(n, pos.shape[0], _c(pos, np.float64), _c(phi, np.float32), out)
+    return out
+
+
+def spline_table(n, eps):
+    d = np.empty((4096, 3), np.float64)
+    s = np.empty((4096, 3), np.float64)
+    lib().or_spline_table(n, eps, d, s)
+    return d, s
+
+
+def tree_force(n, pos, theta=0.3, rsphere=4.0, eps=0.05, variant=VARIANT_B):
+    out = np.empty((pos.shape[0], 3), np.float32)
+    lib().or_tree_force(n, pos.shape[0], _c(pos, np.float64), theta, rsphere, eps, variant, out)
+    return out
+
+
+def direct_short_force(n, pos, targets, rsphere=4.0, eps=0.05):
+    t = _c(targets, np.int64)
+    out = np.empty((t.shape[0], 3), np.float64)
+    lib().or_direct_short_force(n, pos.shape[0], _c(pos, np.float64), rsphere, eps, t.shape[0], t, out)
+    return out
+
+
+def ewald_force(n, pos, targets, eps=0.05, rcut=None, alpha=None, kmax=None):
+    """FP64 periodic Ewald force (reference units) at the target indices."""
+    rcut = rcut if rcut is not None else 0.49 * n
+    alpha = alpha if alpha is not None else 3.6 / rcut
+    if kmax is None:
+        kmax = int(np.ceil(2 * alpha * 3.6 * n / (2 * np.pi)))
+    t = _c(targets, np.int64)
+    out = np.empty((t.shape[0], 3), np.float64)
+    lib().or_ewald_force(n, pos.shape[0], _c(pos, np.float64), eps, t.shape[0], t, rcut, alpha, kmax, out)
+    return out
+
+
+# ------------------------------------------------------- reference (oracle/_ref)
+def ref_pm_force(n, indx, off, efold=0.9):
+    out = np.empty((indx.shape[0], 3), np.float32)
+    ref(VARIANT_A).ref_pm_force(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), efold, out)
+    return out
+
+
+def ref_tree_force(n, indx, off, theta=0.3, rsphere=4.0, eps=0.05, variant=VARIANT_B):
+    out = np.empty((indx.shape[0], 3), np.float32)
+    ref(variant).ref_tree_force(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), theta,
+                                rsphere, eps, out)
+    return out
+
+
+def ref_tsc_density(n, indx, off):
+    out = np.empty(n ** 3, np.float32)
+    ref(VARIANT_A).ref_tsc_density(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), out)
+    return out.reshape(n, n, n)
+
+
+def ref_potential(n, indx, off, efold=0.9):
+    out = np.empty(n ** 3, np.float32)
+    ref(VARIANT_A).ref_potential(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), efold, out)
+    return out.reshape(n, n, n)
+
+
+def ref_spline_table(n, eps):
+    d = np.empty((4096, 3), np.float64)
+    s = np.empty((4096, 3), np.float64)
+    ref(VARIANT_A).ref_spline_table(n, eps, d, s)
+    return d, s
+
+
+def rel_err(f, fref):
+    """Per-particle |f - fref| / |fref|."""
+    num = np.linalg.norm(np.asarray(f, np.float64) - np.asarray(fref, np.float64), axis=1)
+    den = np.linalg.norm(np.asarray(fref, np.float64), axis=1)
+    return num / np.maximum(den, 1e-300)
+
+
+# ------------------------------------------------------------- sort oracle
+AXIS_BITS = 13
+
+
+def cell_bits(n):
+    c = 0
+    while (1 << c) < n:
+        c += 1
+    return max(c, 3)
+
+
+def _spread3(v):
+    x = v.astype(np.uint64) & np.uint64(0x1FFFFF)
+    x = (x | (x << np.uint64(32))) & np.uint64(0x1F00000000FFFF)
+    x = (x | (x << np.uint64(16))) & np.uint64(0x1F0000FF0000FF)
+    x = (x | (x << np.uint64(8))) & np.uint64(0x100F00F00F00F00F)
+    x = (x | (x << np.uint64(4))) & np.uint64(0x10C30C30C30C30C3)
+    x = (x | (x << np.uint64(2))) & np.uint64(0x1249249249249249)
+    return x
+
+
+def morton_keys(pos_u32, n):
+    """39-bit Morton keys of uint32 fixed-point positions: per axis the
+    quantised coordinate q = floor(x_cells * 2^(13 - C)), C = ceil(log2 N)."""
+    sub = AXIS_BITS - cell_bits(n)
+    p = np.asarray(pos_u32, dtype=np.uint64)
+    q = (p * np.uint64(n)) >> np.uint64(32 - sub)
+    return _spread3(q[:, 0]) | (_spread3(q[:, 1]) << np.uint64(1)) | (_spread3(q[:, 2]) << np.uint64(2))
+
+
+def sort_order(keys):
+    """The engine's permutation: stable argsort (ties keep input order)."""
+    return np.argsort(keys, kind="stable")

@@ -1,0 +1,399 @@
+/*
+ * Harness that links the reference's own force-path sources into a CPU
+ * oracle library (oracle/_ref/libref_{A,B}.so). TEST INFRASTRUCTURE ONLY:
+ * tests, the smoke check and bench.py's CPU-baseline leg load it as the
+ * checker; the engine never links or calls it.
+ *
+ * Compiled from the reference tree (not copied):
+ *   Cosmos/pmmain.c, Cosmos/psolver.c, Cosmos/fda4.c, Cosmos/treecorrection.c,
+ *   Cosmos/BasicCell.c, OST/ost.ver2.c, OST/Model4TreeForce.c,
+ *   Timer/timerutil.c
+ * with -DINTEL -DXYZDBL -DGOTPM (sRules.make:32,46) and -fopenmp.
+ *
+ * What this file supplies for a single rank on one box:
+ *  - MPI: the scalar Reduce/Bcast/Barrier calls of the force path become
+ *    copies/no-ops (oracle/stub/mpi.h).
+ *  - FFTW-MPI: fftwf_mpi_execute_dft_r2c / _c2r with the reference's plan
+ *    flags FFTW_MPI_TRANSPOSED_OUT / _IN (FFT/fft.c:130-146): in-place,
+ *    unnormalised, rows padded to 2*(nx/2+1) floats, spectrum stored as
+ *    [y][z][x/2+1] (the layout psolver indexes, Cosmos/psolver.c:49-72).
+ *    The arithmetic is oracle/dft.c in double. The vendored FFTW 3.3.6 is not
+ *    built: it needs its configure-generated config.h.
+ *  - gmigrate (RkS/gmigrate.c:548-580): with one rank it reduces to
+ *    Dump2Outgrid's periodic overlap-add over the 27 box shifts
+ *    (RkS/gmigrate.c:212-273).
+ *  - PaddingParticles (Cosmos/mpirks.sub.c:14-79 -> RkS/mpirks.c:1058-1198):
+ *    with one rank, the periodic images (26 shifts) of every particle that
+ *    fall inside [-w, N+w)^3 with w = RSPHERE, flagged BoundaryGhostflag,
+ *    positions made absolute (shift2pos) and stored in the float x,y,z slots.
+ *  - the side-effect I/O of pmmain (savexzslice, volumeout, CorrMeasure,
+ *    Cosmos/pmmain.c:326,453-456,480-481) is skipped.
+ *
+ * Exported oracle entry points (ref_*) set up a zeroed SimParameters for one
+ * rank owning [0,N)^3, run the reference with PMSTATUS = KICK and
+ * fact2 = 1 on zero velocities, and read the force back from the velocities
+ * (Cosmos/fda4.h:297-299; Cosmos/treecorrection.c:90, OST/ost.ver2.c:273-291).
+ */
+#include <math.h>
+#include <mpi.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+
+#include "eunha.h"
+#include "CosmosEvolFactor.h"
+#include "Model4TreeForce.h"
+#include "dft.h"
+
+/* ------------------------------------------------------------------ MPI */
+static size_t mpi_type_size(MPI_Datatype t) {
+  switch (t) {
+    case MPI_CHAR:
+    case MPI_BYTE: return 1;
+    case MPI_INT:
+    case MPI_FLOAT: return 4;
+    default: return 8;
+  }
+}
+int MPI_Reduce(const void *s, void *r, int n, MPI_Datatype t, MPI_Op op, int root, MPI_Comm c) {
+  (void)op; (void)root; (void)c;
+  if (s != r) memmove(r, s, (size_t)n * mpi_type_size(t));
+  return 0;
+}
+int MPI_Allreduce(const void *s, void *r, int n, MPI_Datatype t, MPI_Op op, MPI_Comm c) {
+  return MPI_Reduce(s, r, n, t, op, 0, c);
+}
+int MPI_Bcast(void *b, int n, MPI_Datatype t, int root, MPI_Comm c) {
+  (void)b; (void)n; (void)t; (void)root; (void)c;
+  return 0;
+}
+int MPI_Barrier(MPI_Comm c) { (void)c; return 0; }
+int MPI_Finalize(void) { return 0; }
+int MPI_Comm_rank(MPI_Comm c, int *r) { (void)c; *r = 0; return 0; }
+int MPI_Comm_size(MPI_Comm c, int *s) { (void)c; *s = 1; return 0; }
+
+/* --------------------------------------------------------- FFTW-MPI shim */
+struct fftwf_plan_s {
+  ptrdiff_t n0, n1, n2; /* z, y, x */
+};
+
+void fftwf_mpi_execute_dft_r2c(fftwf_plan p, float *in, fftwf_complex *out) {
+  ptrdiff_t nz = p->n0, ny = p->n1, nx = p->n2, hx = nx / 2 + 1, mx = 2 * hx;
+  double *r = (double *)malloc(sizeof(double) * nx * ny * nz);
+  double *c = (double *)malloc(sizeof(double) * 2 * hx * ny * nz);
+  for (ptrdiff_t k = 0; k < nz; k++)
+    for (ptrdiff_t j = 0; j < ny; j++)
+      for (ptrdiff_t i = 0; i < nx; i++) r[i + nx * (j + ny * k)] = in[i + mx * (j + ny * k)];
+  odft_r2c_3d(nz, ny, nx, r, c);
+  float *o = (float *)out;
+  /* transposed out: complex element (kx, y, z) at [y][z][kx] */
+  for (ptrdiff_t k = 0; k < nz; k++)
+    for (ptrdiff_t j = 0; j < ny; j++)
+      for (ptrdiff_t i = 0; i < hx; i++) {
+        size_t src = 2 * (i + hx * (j + ny * k));
+        size_t dst = 2 * (i + hx * (k + nz * j));
+        o[dst] = (float)c[src];
+        o[dst + 1] = (float)c[src + 1];
+      }
+  free(r);
+  free(c);
+}
+
+void fftwf_mpi_execute_dft_c2r(fftwf_plan p, fftwf_complex *in, float *out) {
+  ptrdiff_t nz = p->n0, ny = p->n1, nx = p->n2, hx = nx / 2 + 1, mx = 2 * hx;
+  double *c = (double *)malloc(sizeof(double) * 2 * hx * ny * nz);
+  double *r = (double *)malloc(sizeof(double) * nx * ny * nz);
+  const float *ci = (const float *)in;
+  for (ptrdiff_t k = 0; k < nz; k++)
+    for (ptrdiff_t j = 0; j < ny; j++)
+      for (ptrdiff_t i = 0; i < hx; i++) {
+        size_t dst = 2 * (i + hx * (j + ny * k));
+        size_t src = 2 * (i + hx * (k + nz * j));
+        c[dst] = ci[src];
+        c[dst + 1] = ci[src + 1];
+      }
+  odft_c2r_3d(nz, ny, nx, c, r);
+  for (ptrdiff_t k = 0; k < nz; k++)
+    for (ptrdiff_t j = 0; j < ny; j++)
+      for (ptrdiff_t i = 0; i < nx; i++) out[i + mx * (j + ny * k)] = (float)r[i + nx * (j + ny * k)];
+  free(c);
+  free(r);
+}
+
+/* -------------------------------------------------------------- gmigrate */
+void gmigrate(GridInfo *ingrid, GridInfo *outgrid, DoDeInfo *ddinfo, int nddinfo) {
+  (void)ddinfo; (void)nddinfo;
+  ptrdiff_t Nx = ingrid->nx, Ny = ingrid->ny, Nz = ingrid->nz;
+  ptrdiff_t inx = ingrid->jx - ingrid->ix + 1, iny = ingrid->jy - ingrid->iy + 1;
+  ptrdiff_t onx = outgrid->jx - outgrid->ix + 1, ony = outgrid->jy - outgrid->iy + 1,
+            onz = outgrid->jz - outgrid->iz + 1;
+  outgrid->npix = onx * ony * onz;
+  const DenType *src = (const DenType *)(ingrid + 1);
+  DenType *dst = (DenType *)(outgrid + 1);
+  for (int sz = -1; sz <= 1; sz++)
+    for (int sy = -1; sy <= 1; sy++)
+      for (int sx = -1; sx <= 1; sx++) {
+        /* the input grid shifted by s*N, overlapped with the output grid */
+        ptrdiff_t x0 = ingrid->ix + sx * Nx, x1 = ingrid->jx + sx * Nx;
+        ptrdiff_t y0 = ingrid->iy + sy * Ny, y1 = ingrid->jy + sy * Ny;
+        ptrdiff_t z0 = ingrid->iz + sz * Nz, z1 = ingrid->jz + sz * Nz;
+        if (x0 < outgrid->ix) x0 = outgrid->ix;
+        if (y0 < outgrid->iy) y0 = outgrid->iy;
+        if (z0 < outgrid->iz) z0 = outgrid->iz;
+        if (x1 > outgrid->jx) x1 = outgrid->jx;
+        if (y1 > outgrid->jy) y1 = outgrid->jy;
+        if (z1 > outgrid->jz) z1 = outgrid->jz;
+        if (x1 < x0 || y1 < y0 || z1 < z0) continue;
+        for (ptrdiff_t k = z0; k <= z1; k++)
+          for (ptrdiff_t j = y0; j <= y1; j++)
+            for (ptrdiff_t i = x0; i <= x1; i++) {
+              ptrdiff_t io = (i - outgrid->ix) + onx * ((j - outgrid->iy) + ony * (k - outgrid->iz));
+              ptrdiff_t ii = (i - sx * Nx - ingrid->ix) +
+                             inx * ((j - sy * Ny - ingrid->iy) + iny * (k - sz * Nz - ingrid->iz));
+              dst[io] += src[ii];
+            }
+      }
+}
+
+/* ------------------------------------------------------ PaddingParticles */
+void PaddingParticles(SimParameters *simpar) {
+  double N[3] = {(double)NX(simpar), (double)NY(simpar), (double)NZ(simpar)};
+  double w = RSPHERE(simpar);
+  NXNY(simpar) = NX(simpar) * NY(simpar);
+  ptrdiff_t np = DM_NP(simpar), cap = 1024, n = 0;
+  treedmparticletype *pad = (treedmparticletype *)malloc(sizeof(treedmparticletype) * cap);
+  treedmparticletype *bp = DM_TBP(simpar);
+  for (ptrdiff_t i = 0; i < np; i++) {
+    double x[3] = {XofP(simpar, bp + i), YofP(simpar, bp + i), ZofP(simpar, bp + i)};
+    for (int s = 0; s < 27; s++) {
+      int sh[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
+      if (sh[0] == 0 && sh[1] == 0 && sh[2] == 0) continue;
+      double y[3];
+      int inside = 1;
+      for (int d = 0; d < 3; d++) {
+        y[d] = x[d] + sh[d] * N[d];
+        if (!(y[d] >= -w && y[d] < N[d] + w)) inside = 0;
+      }
+      if (!inside) continue;
+      if (n == cap) {
+        cap *= 2;
+        pad = (treedmparticletype *)realloc(pad, sizeof(treedmparticletype) * cap);
+      }
+      pad[n] = bp[i];
+      pad[n].x = (float)y[0];
+      pad[n].y = (float)y[1];
+      pad[n].z = (float)y[2];
+      CLEAR_FLAG(pad + n);
+      SET_FLAG(pad + n, BoundaryGhostflag);
+      SET_FLAG(pad + n, DMflag);
+      n++;
+    }
+  }
+  DM_TBPP(simpar) = pad;
+  DM_NPAD(simpar) = n;
+  SPH_NPAD(simpar) = VORO_NPAD(simpar) = STAR_NPAD(simpar) = AGN_NPAD(simpar) = 0;
+}
+
+/* ---------------------------------------------- skipped side effects */
+void CorrMeasure(SimParameters *simpar, GridInfo *g) { (void)simpar; (void)g; }
+void savexzslice(SimParameters *simpar, DenType *d) { (void)simpar; (void)d; }
+void volumeout(SimParameters *simpar, GridInfo *g, int which) { (void)simpar; (void)g; (void)which; }
+float GetFact1(SimParameters *simpar, float a, float b) {
+  (void)simpar; (void)a; (void)b;
+  fprintf(stderr, "oracle/_ref: GetFact1 (PUSH status) is not part of the oracle harness\n");
+  abort();
+}
+
+/* ------------------------------------------------------- oracle set-up */
+extern int initflag; /* Cosmos/treecorrection.c:221: spline table built once */
+extern FORCEARRAYTYPE diff[NSPLINE][3], slope[NSPLINE][3]; /* OST/Model4TreeForce.c:14 */
+void pmmain(SimParameters *, EvolFact);
+void treecorrection(SimParameters *, DeterminedEvolFact *);
+void *MakeDenGrid4TSC(SimParameters *, GridInfo *, ptrdiff_t, ptrdiff_t);
+void TSC(SimParameters *, GridInfo *);
+GridInfo *MakeGrids4FFTWDD(SimParameters *, GridInfo *);
+void psolver(SimParameters *, GridInfo *);
+void i_force_spline(SimParameters *);
+
+typedef struct {
+  SimParameters sim;
+  DoDeInfo dd;
+  struct fftwf_plan_s fplan, bplan;
+} RefBox;
+
+static RefBox *refbox_new(int n, float efold, float eps, float theta, float rsphere) {
+  RefBox *b = (RefBox *)calloc(1, sizeof(RefBox));
+  SimParameters *s = &b->sim;
+  NX(s) = n;
+  s->fftwgrid.gridinfo.ny = n;
+  s->fftwgrid.gridinfo.nz = n;
+  NXNY(s) = (ptrdiff_t)n * n;
+  MYID(s) = 0;
+  NID(s) = 1;
+  MPI_COMM(s) = MPI_COMM_WORLD;
+  LOCAL_NZ(s) = n;
+  LOCAL_Z_START(s) = 0;
+  LOCAL_GRID_SIZE(s) = (ptrdiff_t)n * n * (n / 2 + 1);
+  LOCAL_NY_AFTER_TRANSPOSE(s) = n;
+  LOCAL_Y_START_AFTER_TRANSPOSE(s) = 0;
+  b->fplan.n0 = b->fplan.n1 = b->fplan.n2 = n;
+  b->bplan = b->fplan;
+  FFTW_F_PLAN(s) = &b->fplan;
+  FFTW_B_PLAN(s) = &b->bplan;
+  for (int d = 0; d < 3; d++) {
+    b->dd.lgroup.r.rmin[d] = 0;
+    b->dd.lgroup.r.rmax[d] = n;
+  }
+  NDDINFO(s) = 1;
+  DM_DDINFO(s) = &b->dd;
+  TDM_DDINFO(s) = &b->dd;
+  s->bp.dm.mass = 1.0f; /* cosmology.c:268 */
+  GRV_EFOLD(s) = efold;
+  GRV_EPSILON(s) = eps;
+  THETA(s) = theta;
+  RSPHERE(s) = rsphere;
+  PMSTATUS(s) = KICK;
+  STEPCOUNT(s) = 100;
+  ANOW(s) = 1.0;
+  ASTEP(s) = 0.0;
+  return b;
+}
+
+static void set_index(indxflag *u, uint64_t idx) {
+  u->indx = idx & ((((uint64_t)1) << 56) - 1);
+}
+
+/* Reference PM force (pmmain with KICK, fact2 = 1) on particles given as
+ * Lagrangian index + float offset (XYZDBL, eunha.h:1228-1232). */
+int ref_pm_force(int n, int64_t np, const uint64_t *indx, const float *off, float efold,
+                 float *force) {
+  RefBox *b = refbox_new(n, efold, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  dmparticletype *p = (dmparticletype *)calloc((size_t)np, sizeof(dmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    set_index(&p[i].u4if, indx[i]);
+    p[i].x = off[3 * i];
+    p[i].y = off[3 * i + 1];
+    p[i].z = off[3 * i + 2];
+  }
+  DM_NP(s) = np;
+  DM_BP(s) = p;
+  EvolFact ef;
+  memset(&ef, 0, sizeof(ef));
+  ef.fact2 = 1.0f;
+  pmmain(s, ef);
+  for (int64_t i = 0; i < np; i++) {
+    force[3 * i] = p[i].vx;
+    force[3 * i + 1] = p[i].vy;
+    force[3 * i + 2] = p[i].vz;
+  }
+  free(p);
+  free(b);
+  return 0;
+}
+
+/* Reference short-range tree correction (treecorrection, fact2 = 1). */
+int ref_tree_force(int n, int64_t np, const uint64_t *indx, const float *off, float theta,
+                   float rsphere, float eps, float *force) {
+  RefBox *b = refbox_new(n, 0.9f, eps, theta, rsphere);
+  SimParameters *s = &b->sim;
+  treedmparticletype *p = (treedmparticletype *)calloc((size_t)np, sizeof(treedmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    set_index(&p[i].u4if, indx[i]);
+    p[i].x = off[3 * i];
+    p[i].y = off[3 * i + 1];
+    p[i].z = off[3 * i + 2];
+  }
+  DM_NP(s) = np;
+  DM_TBP(s) = p;
+  DeterminedEvolFact ef[1];
+  ef[0].fact1 = 1.0f;
+  ef[0].fact2 = 1.0f;
+  initflag = 0; /* rebuild the table for this N and softening */
+  treecorrection(s, ef);
+  for (int64_t i = 0; i < np; i++) {
+    force[3 * i] = p[i].vx;
+    force[3 * i + 1] = p[i].vy;
+    force[3 * i + 2] = p[i].vz;
+  }
+  free(p);
+  free(b);
+  return 0;
+}
+
+/* Folded TSC density contrast (mesh - 1), [z][y][x], as it enters the r2c. */
+int ref_tsc_density(int n, int64_t np, const uint64_t *indx, const float *off, float *mesh) {
+  RefBox *b = refbox_new(n, 0.9f, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  dmparticletype *p = (dmparticletype *)calloc((size_t)np, sizeof(dmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    set_index(&p[i].u4if, indx[i]);
+    p[i].x = off[3 * i];
+    p[i].y = off[3 * i + 1];
+    p[i].z = off[3 * i + 2];
+  }
+  DM_NP(s) = np;
+  DM_BP(s) = p;
+  GridInfo *dengrid = (GridInfo *)malloc(sizeof(GridInfo));
+  dengrid = (GridInfo *)MakeDenGrid4TSC(s, dengrid, 1, 2);
+  TSC(s, dengrid);
+  GridInfo *fg = MakeGrids4FFTWDD(s, dengrid);
+  const float *d = (const float *)(fg + 1);
+  ptrdiff_t mx = 2 * (n / 2 + 1);
+  for (ptrdiff_t k = 0; k < n; k++)
+    for (ptrdiff_t j = 0; j < n; j++)
+      for (ptrdiff_t i = 0; i < n; i++) mesh[i + n * (j + (ptrdiff_t)n * k)] = d[i + mx * (j + n * k)];
+  free(fg);
+  free(dengrid);
+  free(p);
+  free(b);
+  return 0;
+}
+
+/* Potential after psolver and the c2r, [z][y][x] (before the fda4 ghosting). */
+int ref_potential(int n, int64_t np, const uint64_t *indx, const float *off, float efold,
+                  float *phi) {
+  RefBox *b = refbox_new(n, efold, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  dmparticletype *p = (dmparticletype *)calloc((size_t)np, sizeof(dmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    set_index(&p[i].u4if, indx[i]);
+    p[i].x = off[3 * i];
+    p[i].y = off[3 * i + 1];
+    p[i].z = off[3 * i + 2];
+  }
+  DM_NP(s) = np;
+  DM_BP(s) = p;
+  GridInfo *dengrid = (GridInfo *)malloc(sizeof(GridInfo));
+  dengrid = (GridInfo *)MakeDenGrid4TSC(s, dengrid, 1, 2);
+  TSC(s, dengrid);
+  GridInfo *fg = MakeGrids4FFTWDD(s, dengrid);
+  float *d = (float *)(fg + 1);
+  fftwf_mpi_execute_dft_r2c(FFTW_F_PLAN(s), d, (fftwf_complex *)d);
+  psolver(s, fg);
+  fftwf_mpi_execute_dft_c2r(FFTW_B_PLAN(s), (fftwf_complex *)d, d);
+  ptrdiff_t mx = 2 * (n / 2 + 1);
+  for (ptrdiff_t k = 0; k < n; k++)
+    for (ptrdiff_t j = 0; j < n; j++)
+      for (ptrdiff_t i = 0; i < n; i++) phi[i + n * (j + (ptrdiff_t)n * k)] = d[i + mx * (j + n * k)];
+  free(fg);
+  free(dengrid);
+  free(p);
+  free(b);
+  return 0;
+}
+
+/* The short-range force table (OST/Model4TreeForce.c:48-91) for this N and
+ * softening: diff and slope, NSPLINE x 3 doubles each. */
+int ref_spline_table(int n, float eps, double *diff_out, double *slope_out) {
+  RefBox *b = refbox_new(n, 0.9f, eps, 0.3f, 4.0f);
+  i_force_spline(&b->sim);
+  memcpy(diff_out, diff, sizeof(double) * NSPLINE * 3);
+  memcpy(slope_out, slope, sizeof(double) * NSPLINE * 3);
+  free(b);
+  return 0;
+}
+
+int ref_nspline(void) { return NSPLINE; }
