@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""TreePM force-evaluation benchmark.
+
+One step = one full TreePM force evaluation (Morton sort, TSC deposit,
+Poisson FFT, fda4 gradient + interpolation, tree build, tree walk, forces
+scattered back to the caller's order) of the clustered 256^3 workload:
+256^3 particles on a 256^3 mesh, L = 200 Mpc/h, Zel'dovich field with
+P(k) ~ k^-2 exp(-(0.5k)^2) and 1.5-spacing rms displacement plus 200 Plummer
+spheres (a = 0.64 cells, 2000-20000 particles each), softening 0.05 cells,
+theta 0.3, rsphere 4, efold 0.9 (the reference's law).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+value: Mparticles/s over all ranks with the positions resident in HBM.
+e2e:   the same metric through the public C ABI with pinned host buffers
+       (positions uploaded and forces read back every step).
+With N > 1 (torchrun), every rank evaluates its own independent box (replicas,
+weak scaling); no collective is on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mparticles/s per TreePM force eval (plain vs batched) at rms err≤1e-3; p50/p99 latency"
+UNIT = "Mparticles/s"
+EPS = 0.05
+FP32_LANES_PER_SM = 128
+# FLOPs charged per evaluated interaction of the walk (DESIGN.md derives them):
+# particle-particle 20, particle-node (quadrupole) 65
+FLOP_PP, FLOP_PC = 20, 65
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _clock_sampler(path):
+    fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except (FileNotFoundError, OSError):
+        return None
+
+
+def _clock_summary(path, device):
+    sms, maxs, reasons = [], [], set()
+    try:
+        for line in open(path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(device):
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxs.append(float(parts[2]))
+            except ValueError:
+                continue
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+    except OSError:
+        pass
+    if not sms:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
+            "samples": len(sms)}
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the profiled kernels, from the committed ncu
+    summary (profiles/ncu_traffic.txt: '<kernel> <bytes_per_launch> <units>')."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "ncu_traffic.txt")):
+            p = line.split()
+            if len(p) >= 3 and not line.startswith("#"):
+                out[p[0]] = (float(p[1]), float(p[2]))
+    except OSError:
+        pass
+    return out
+
+
+# ---------------------------------------------------------------- CPU arms
+def reference_sample():
+    """The bounded CPU sample: the same clustered workload at 128^3 (2.1M
+    particles, 25 Plummer spheres of 2000-20000 particles with the same scale
+    radius, so the same local densities), one PM + tree-correction
+    evaluation through the reference's own pmmain/treecorrection."""
+    from lageunha_b200 import ic
+    return ic.workload("clustered256", scale=128)
+
+
+def run_reference_eval(ps):
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    O.ref_pm_force(ps.n_mesh, ps.indx, ps.offset, 0.9)
+    O.ref_tree_force(ps.n_mesh, ps.indx, ps.offset, theta=0.3, rsphere=4.0, eps=EPS, variant=O.VARIANT_A)
+    return time.perf_counter() - t0
+
+
+def _quiet_stdout():
+    """The reference prints its stage timers; keep the JSON line alone on stdout."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    os.close(devnull)
+    return saved
+
+
+def _restore_stdout(saved):
+    sys.stdout.flush()
+    os.dup2(saved, 1)
+    os.close(saved)
+
+
+def cpu_baseline():
+    ps = reference_sample()
+    saved = _quiet_stdout()
+    try:
+        dt = run_reference_eval(ps)
+    finally:
+        _restore_stdout(saved)
+    return {"value": ps.np / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"clustered workload at 128^3 ({ps.np} particles, 25 Plummer spheres), one "
+                      f"pmmain + treecorrection of the reference built from its sources (variant A), "
+                      f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s"}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    if not O.ref_available(O.VARIANT_A):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_A.so was not built "
+                          "(the reference tree was absent when the oracle was compiled)"}))
+        return 0
+    ps = reference_sample()
+    saved = _quiet_stdout()
+    try:
+        for _ in range(args.warmup):
+            run_reference_eval(ps)
+        times = [run_reference_eval(ps) for _ in range(args.steps)]
+    finally:
+        _restore_stdout(saved)
+    tot = sum(times)
+    value = ps.np * args.steps / tot / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Zel'dovich + Plummer spheres)",
+        "config": {"workload": "clustered, bounded CPU sample at 128^3", "n_mesh": 128, "particles": ps.np,
+                   "theta": 0.3, "rsphere": 4.0, "epsilon": EPS, "efold": 0.9},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"{ps.np} particles (clustered 128^3) per step, reference pmmain + "
+                                   f"treecorrection (variant A) on {os.cpu_count()} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- engine arm
+def run_engine_arm(args):
+    import torch
+    from lageunha_b200 import engine as E
+    from lageunha_b200 import ic
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    ps = ic.workload(args.workload, scale=args.scale)
+    n = ps.n_mesh
+    pu = ps.positions_u32()
+    npart = ps.np
+
+    eng = E.Engine(n, epsilon=EPS, theta=0.3, rsphere=4.0, efold=0.9, device=local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    pos_dev = torch.from_numpy(pu.view(np.int32)).to(f"cuda:{local}")
+    f_dev = torch.empty((npart, 3), dtype=torch.float32, device=f"cuda:{local}")
+    eng.load_fixed(pos_dev)
+
+    def step_dev():
+        eng.compute(E.PART_ALL)
+        eng.forces(f_dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step_dev()
+    launches = eng.launch_count() + 1  # compute + the scatter to caller order
+    stages = {k: 0.0 for k in E.STAGES}
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"tpm_clocks_{rank}.csv")
+    sampler = _clock_sampler(clk_path)
+    time.sleep(0.3)
+    barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    per_step = []
+    t_start.record(stream)
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step_dev()
+        b.record(stream)
+        per_step.append((a, b))
+        st = eng.stage_times()
+        for k in stages:
+            stages[k] += st.get(k, 0.0)
+    t_end.record(stream)
+    barrier()
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    ms_total = t_start.elapsed_time(t_end)
+    lat = [a.elapsed_time(b) for a, b in per_step]
+    counters = eng.counters()
+    ms_max = ms_total
+    if dist is not None:
+        t = torch.tensor([ms_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = ws * npart / (ms_step * 1e-3) / 1e6
+
+    # ---- e2e: host buffers through the public API, copies in the timed region
+    pos_host = torch.from_numpy(pu.view(np.int32).copy()).pin_memory()
+    f_host = torch.empty((npart, 3), dtype=torch.float32).pin_memory()
+
+    def step_e2e():
+        eng.load_fixed(pos_host)
+        eng.compute(E.PART_ALL)
+        eng.forces(f_host)
+
+    step_e2e()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e1.record(stream)
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = ws * npart * args.steps / (ms_e2e * 1e-3) / 1e6
+
+    # ---- accuracy against the FP64 Ewald sum on a 4096-particle subsample (untimed)
+    err = None
+    if not args.no_ewald:
+        fh = f_host.numpy()
+        rng = np.random.Generator(np.random.PCG64(4096))
+        tg = np.sort(rng.choice(npart, 4096, replace=False)).astype(np.int64)
+        few = eng.ewald(tg)
+        e = np.linalg.norm(fh[tg].astype(np.float64) - few, axis=1) / np.linalg.norm(few, axis=1)
+        err = {"rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)), "targets": 4096}
+
+    clocks = _clock_summary(clk_path, local)
+    peaks = _peaks()
+
+    # ---- roofline of the dominant kernel
+    per = {k: v / args.steps for k, v in stages.items()}
+    dominant = max(per, key=per.get)
+    sm_max = clocks.get("sm_max_mhz") or peaks.get("sm_max_mhz") or 1965.0
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = nsm * FP32_LANES_PER_SM * 2 * sm_max * 1e6 / 1e12
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = _ncu_traffic()
+    if dominant == "tree_walk":
+        flops = FLOP_PP * counters["pp"] + FLOP_PC * counters["pc"]
+        achieved = flops / (per["tree_walk"] * 1e-3) / 1e12
+        tr = traffic.get("k_tree_walk")
+        roofline = {"bound": "fp32", "kernel": "k_tree_walk", "achieved": achieved, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                    "peak_source": f"nominal FP32 {nsm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                                   "(no measured FP32 figure; HBM peak of measured)",
+                    "traffic": (tr[0] * npart / tr[1]) if tr else None,
+                    "algorithmic": f"{FLOP_PP} flop per particle-particle and {FLOP_PC} per particle-node "
+                                   f"interaction evaluated: {counters['pp']} and {counters['pc']} per launch"}
+    else:
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": None, "peak": hbm_peak, "unit": "GB/s"}
+    # HBM-bound stages: algorithmic bytes per particle
+    bytes_pp = {"sort": 28 + 5 * 32, "deposit": 16, "fft": 16 * n ** 3 / npart, "fda4": 28}
+    hbm_stages = {}
+    for k, b in bytes_pp.items():
+        if per.get(k, 0) > 0:
+            gbs = b * npart / (per[k] * 1e-3) / 1e9
+            hbm_stages[k] = {"ms": per[k], "GB/s": gbs, "frac": gbs / hbm_peak}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Zel'dovich field + Plummer spheres; no dataset)",
+        "config": {"workload": args.workload + (f" at {n}^3" if args.scale else "") +
+                               " (one TreePM force evaluation per step, plain engine)",
+                   "n_mesh": n, "particles_per_gpu": npart, "theta": 0.3, "rsphere": 4.0, "epsilon": EPS,
+                   "efold": 0.9, "law": "reference",
+                   "l2": f"inputs larger than L2: {12 * npart / 1e6:.0f} MB of positions, "
+                         f"{4 * n ** 3 / 1e6:.0f} MB mesh",
+                   "parallelism": f"replicas x{ws}"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "stage_ms": per,
+        "hbm_stages": hbm_stages,
+        "counters": counters,
+        "err_vs_ewald": err,
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * npart,
+                "d2h_bytes_per_step": 12 * npart},
+        "gpu_launches": launches * args.steps,
+        "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
+                   "reasons": clocks.get("reasons", [])},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="clustered256", choices=["clustered256", "plain64", "scale512"])
+    ap.add_argument("--scale", type=int, default=None,
+                    help="mesh size of a smaller instance of the workload (profiling captures)")
+    ap.add_argument("--no-ewald", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_engine_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -2,6 +2,7 @@
 // include/tpm_engine.h.
 #include <math.h>
 #include <stdarg.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -21,6 +22,17 @@ using namespace tpm;
 
 static thread_local std::string g_err;
 
+// TPM_DEBUG_SYNC=1 synchronises and checks after every stage of a force
+// evaluation, so a failing kernel is reported by stage name.
+static bool debug_sync() {
+  static int v = -1;
+  if (v < 0) {
+    const char *s = getenv("TPM_DEBUG_SYNC");
+    v = (s && s[0] == '1') ? 1 : 0;
+  }
+  return v == 1;
+}
+
 static int fail(int code, const char *fmt, ...) {
   char buf[512];
   va_list ap;
@@ -38,6 +50,13 @@ static int fail(int code, const char *fmt, ...) {
       return fail(e_ == cudaErrorMemoryAllocation ? TPM_E_NOMEM : TPM_E_CUDA, "%s: %s (%s:%d)", #call, \
                   cudaGetErrorString(e_), __FILE__, __LINE__);                          \
   } while (0)
+
+static cudaError_t stage_check(cudaStream_t st, const char *name) {
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && debug_sync()) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) fprintf(stderr, "tpm: stage %s failed: %s\n", name, cudaGetErrorString(e));
+  return e;
+}
 
 enum Stage { kStSort = 0, kStDeposit, kStFft, kStFda4, kStTreeBuild, kStTreeWalk, kStFinish, kNStages };
 
@@ -110,7 +129,9 @@ static int check_params(const tpm_params *p) {
   if (p->law != TPM_LAW_REFERENCE && p->law != TPM_LAW_GAUSSIAN) return fail(TPM_E_ARG, "unknown law %d", p->law);
   if (!(p->theta > 0.f && p->theta < 1.f)) return fail(TPM_E_ARG, "theta %g outside (0,1)", p->theta);
   if (!(p->rsphere > 0.f && p->rsphere <= 6.0f)) return fail(TPM_E_ARG, "rsphere %g outside (0, 6]", p->rsphere);
-  if (p->rsphere * 4.f >= (float)p->n_mesh) return fail(TPM_E_ARG, "rsphere %g too large for n_mesh %d", p->rsphere, p->n_mesh);
+  // pairs are taken at their minimum image, so the cutoff sphere must fit in
+  // half the box
+  if (p->rsphere * 2.f >= (float)p->n_mesh) return fail(TPM_E_ARG, "rsphere %g too large for n_mesh %d", p->rsphere, p->n_mesh);
   if (!(p->epsilon >= 0.f)) return fail(TPM_E_ARG, "epsilon %g < 0", p->epsilon);
   if (p->law == TPM_LAW_GAUSSIAN && !(p->rs_split > 0.f)) return fail(TPM_E_ARG, "rs_split must be > 0");
   if (!(p->particle_mass > 0.f)) return fail(TPM_E_ARG, "particle_mass must be > 0");
@@ -232,12 +253,15 @@ static int alloc_mesh(tpm_ctx *c) {
   fft_plan_init(c->fp, g.n);
   if (make_phi_tensor_map(g, c->phi, &c->tmap) != 0) return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
   CK(cudaGetLastError());
+  // set-up work above ran on the legacy stream; the context stream is
+  // non-blocking, so finish it before any force evaluation
+  CK(cudaDeviceSynchronize());
   return 0;
 }
 
 static void free_particles(tpm_ctx *c) {
   void *ps[] = {c->pos, c->vel, c->key, c->key_alt, c->val, c->val_alt, c->spos, c->fpm, c->ftree, c->fout,
-                c->ss.hist, c->tb.start, c->tb.count, c->tb.child, c->tb.nchild, c->tb.level, c->tb.geo,
+                c->ss.hist, c->ss.dtotal, c->tb.start, c->tb.count, c->tb.child, c->tb.nchild, c->tb.level, c->tb.geo,
                 c->tb.mom0, c->tb.mom1, c->tb.mom2, c->tb.tile_sum, c->tb.groups};
   for (void *p : ps)
     if (p) cudaFree(p);
@@ -248,6 +272,7 @@ static void free_particles(tpm_ctx *c) {
   c->spos = nullptr;
   c->fpm = c->ftree = c->fout = nullptr;
   c->ss.hist = nullptr;
+  c->ss.dtotal = nullptr;
   c->tb.start = c->tb.count = c->tb.child = c->tb.nchild = nullptr;
   c->tb.level = nullptr;
   c->tb.geo = nullptr;
@@ -273,6 +298,7 @@ static int ensure_particles(tpm_ctx *c, int64_t np) {
   CK(cudaMalloc(&c->fout, sizeof(float) * 3 * cap));
   int64_t ntiles = sort_tiles(cap);
   CK(cudaMalloc(&c->ss.hist, sizeof(uint32_t) * 256 * (ntiles + 1)));
+  CK(cudaMalloc(&c->ss.dtotal, sizeof(uint32_t) * 256));
   c->ss.cap_tiles = ntiles;
   // tree: every node holds >= 1 particle and every inner node >= 10, so the
   // node count is bounded by the leaves (<= np) plus the inner nodes
@@ -556,6 +582,7 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
   c->perm = v;
   launch_gather_pos(c->pos, c->perm, np, c->spos, st);
   c->launches += 2;
+  CK(stage_check(st, "sort"));
   CK(cudaEventRecord(c->ev[1], st));
   // ---- PM
   if (parts & TPM_PART_PM) {
@@ -564,11 +591,14 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
     launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st);
     c->launches += 2;
+    CK(stage_check(st, "deposit"));
     CK(cudaEventRecord(c->ev[2], st));
     launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st, &c->launches);
+    CK(stage_check(st, "fft"));
     CK(cudaEventRecord(c->ev[3], st));
     launch_fda4(g, &c->tmap, c->phi, c->spos, c->tile_start, c->fpm, c->err, st);
     c->launches += 1;
+    CK(stage_check(st, "fda4"));
     CK(cudaEventRecord(c->ev[4], st));
   } else {
     for (int i = 2; i <= 4; i++) CK(cudaEventRecord(c->ev[i], st));
@@ -585,8 +615,10 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     tree_build(tp, c->skey, c->spos, np, c->tb, c->err, st, &c->launches);
     CK(cudaMemsetAsync(c->tb.counters, 0, sizeof(uint32_t) * 16, st));
     tree_groups(tp, c->skey, np, c->tb, c->cube_start, c->ncubes, 3 * (g.sub_bits + 2), st, &c->launches);
+    CK(stage_check(st, "tree_build"));
     CK(cudaEventRecord(c->ev[5], st));
     tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
+    CK(stage_check(st, "tree_walk"));
     CK(cudaEventRecord(c->ev[6], st));
   } else {
     for (int i = 5; i <= 6; i++) CK(cudaEventRecord(c->ev[i], st));
