@@ -164,7 +164,8 @@ int tpm_ewald(tpm_ctx *ctx, int64_t nt, const int64_t *targets, double *out);
 int tpm_stage_times(tpm_ctx *ctx, float *ms, int n);
 
 /* Counters of the last force evaluation: [0] tree nodes, [1] particle-
- * particle interactions, [2] particle-node interactions, [3] walk groups. */
+ * particle interactions, [2] particle-node interactions, [3] walk groups,
+ * [4] walk iterations, [5] nodes examined by the walk, [6] deepest walk stack. */
 int tpm_counters(tpm_ctx *ctx, int64_t *out, int n);
 
 /* Kernel launches issued by the last tpm_compute_forces. */

@@ -9,7 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/tpm_engine.h"
+#include "tpm_engine.h"
 #include "engine_internal.cuh"
 
 namespace tpm {
@@ -102,7 +102,7 @@ struct tpm_ctx {
   float stage_ms[kNStages];
   unsigned stage_mask = 0;
   int64_t launches = 0;
-  int64_t counters[4] = {0, 0, 0, 0};
+  int64_t counters[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 extern "C" {
@@ -167,7 +167,7 @@ static double law_f(int kind, double r, float eps, double rs, double LL) {
 
 static int build_law(tpm_ctx *c) {
   const tpm_params &p = c->prm;
-  if (c->law.t01 && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
+  if (c->law.t0 && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
       c->law_rs == p.rs_split && c->law_rsphere == p.rsphere)
     return 0;
   const int NS = 4096;
@@ -197,20 +197,23 @@ static int build_law(tpm_ctx *c) {
   }
   int entries = (int)(p.rsphere * invran) + 2;
   if (entries > NS) entries = NS;
-  std::vector<float4> t01(entries);
-  std::vector<float2> t2(entries + 1);
+  std::vector<float2> t0(entries + 1);
+  std::vector<float4> t12(entries);
   for (int i = 0; i < entries; i++) {
-    t01[i] = make_float4((float)diff[3 * i], (float)slope[3 * i], (float)diff[3 * i + 1], (float)slope[3 * i + 1]);
-    t2[i] = make_float2((float)diff[3 * i + 2], (float)slope[3 * i + 2]);
+    double dl = ran2nran;
+    t0[i] = make_float2((float)diff[3 * i], (float)(slope[3 * i] * dl));
+    t12[i] = make_float4((float)diff[3 * i + 1], (float)(slope[3 * i + 1] * dl), (float)diff[3 * i + 2],
+                         (float)(slope[3 * i + 2] * dl));
   }
-  if (c->law.t01) cudaFree(c->law.t01);
-  if (c->law.t2) cudaFree(c->law.t2);
-  c->law.t01 = nullptr;
-  c->law.t2 = nullptr;
-  CK(cudaMalloc(&c->law.t01, sizeof(float4) * entries));
-  CK(cudaMalloc(&c->law.t2, sizeof(float2) * (entries + 1)));
-  CK(cudaMemcpy(c->law.t01, t01.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->law.t2, t2.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
+  t0[entries] = make_float2(0.f, 0.f);
+  if (c->law.t0) cudaFree(c->law.t0);
+  if (c->law.t12) cudaFree(c->law.t12);
+  c->law.t0 = nullptr;
+  c->law.t12 = nullptr;
+  CK(cudaMalloc(&c->law.t0, sizeof(float2) * (entries + 1)));
+  CK(cudaMalloc(&c->law.t12, sizeof(float4) * entries));
+  CK(cudaMemcpy(c->law.t0, t0.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->law.t12, t12.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
   c->law.entries = entries;
   c->law.delta = ran2nran;
   c->law.inv_delta = invran;
@@ -468,8 +471,8 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   free_particles(c);
   free_mesh(c);
-  if (c->law.t01) cudaFree(c->law.t01);
-  if (c->law.t2) cudaFree(c->law.t2);
+  if (c->law.t0) cudaFree(c->law.t0);
+  if (c->law.t12) cudaFree(c->law.t12);
   if (c->err) cudaFree(c->err);
   if (c->tb.counters) cudaFree(c->tb.counters);
   if (c->tb.level_range) cudaFree(c->tb.level_range);
@@ -642,7 +645,7 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
   }
   // counters: nodes, pp, pc, groups
   {
-    uint32_t hc[6];
+    uint32_t hc[12];
     uint32_t lr[2 * (kAxisBits + 2)];
     cudaMemcpy(hc, c->tb.counters, sizeof(hc), cudaMemcpyDeviceToHost);
     cudaMemcpy(lr, c->tb.level_range, sizeof(lr), cudaMemcpyDeviceToHost);
@@ -653,6 +656,9 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     c->counters[1] = (int64_t)(((uint64_t)hc[3] << 32) | hc[2]);
     c->counters[2] = (int64_t)(((uint64_t)hc[5] << 32) | hc[4]);
     c->counters[3] = hc[0];
+    c->counters[4] = (int64_t)(((uint64_t)hc[7] << 32) | hc[6]);
+    c->counters[5] = (int64_t)(((uint64_t)hc[9] << 32) | hc[8]);
+    c->counters[6] = hc[10];
   }
   c->parts_valid = parts & TPM_PART_ALL;
   return 0;
@@ -793,7 +799,7 @@ int tpm_stage_times(tpm_ctx *c, float *ms, int n) {
 
 int tpm_counters(tpm_ctx *c, int64_t *out, int n) {
   if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
-  int k = n < 4 ? n : 4;
+  int k = n < 7 ? n : 7;
   for (int i = 0; i < k; i++) out[i] = c->counters[i];
   return k;
 }

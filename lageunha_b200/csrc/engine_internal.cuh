@@ -108,10 +108,13 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
 void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
                  uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
                  int64_t *launches);
-// Short-range law table: float4 {d0, s0, d1, s1} and float2 {d2, s2} per entry.
+// Short-range law table in index units: at w = r / delta, entry n = floor(w)
+// and frac = w - n, column c is diff_c[n] + slope_c[n]*delta*frac
+// (OST/Model4TreeForce.c:34-46). t0 = {diff0, slope0*delta},
+// t12 = {diff1, slope1*delta, diff2, slope2*delta}.
 struct LawTable {
-  float4 *t01 = nullptr;
-  float2 *t2 = nullptr;
+  float2 *t0 = nullptr;
+  float4 *t12 = nullptr;
   int entries = 0;
   float delta = 0, inv_delta = 0;
 };

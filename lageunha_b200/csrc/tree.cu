@@ -448,7 +448,7 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 }
 
 // ------------------------------------------------------------------ walk
-constexpr int kWalkWarps = 8;
+constexpr int kWalkWarps = 16;
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kStackCap = 8192;
 constexpr int kListCap = 64;
@@ -456,131 +456,161 @@ constexpr int kListCap = 64;
 struct WarpLists {
   uint32_t pc[kListCap];
   uint32_t pp[kListCap];
-  float stage[32 * 12];
+  float4 stage[32 * 3];  // PP: one float4 per source; PC: three per node
 };
 
 struct WalkCtx {
   float tx, ty, tz;       // this lane's target relative to u_ref
-  float ax, ay, az;       // accumulated force
+  float ax, ay, az;       // particle-particle sum (without the particle mass)
+  float bx, by, bz;       // particle-node sum
   bool active;
   uint32_t rx, ry, rz;    // u_ref
 };
 
+// Hardware reciprocal square root (MUFU), flushing denormals: the walk's
+// distances are at least 2^-32 cells apart or exactly zero.
+TPM_D float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Table lookup at w = r/delta (w >= 0) without float<->int conversions:
+// adding 1.5*2^23 rounding toward -inf leaves floor(w) in the low mantissa.
+TPM_D int table_index(float w, float &frac) {
+  const float magic = 12582912.0f;
+  float v = __fadd_rd(w, magic);
+  float fl = v - magic;
+  frac = w - fl;
+  return __float_as_int(v) - 0x4B400000;
+}
+
+// One source against this lane's target: the reference's AddPar
+// (OST/ost.ver2.c:279-293) without the mass factor, masked to r^2 <= rs^2.
+// Coordinates are in table-index units (cells / delta); r2 = 0 (the target
+// itself) gives rsqrt = inf, w = NaN, which fminf turns into wmax, and a zero
+// separation, so it adds nothing.
+TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, const float2 *__restrict__ t0,
+                   float &ax, float &ay, float &az) {
+  float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
+  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float wq = fminf(r2 * rsqrt_approx(r2), wmax);
+  float frac;
+  int nt = table_index(wq, frac);
+  float2 c = t0[nt];
+  float f = fmaf(c.y, frac, c.x);
+  f = r2 <= rs2 ? f : 0.f;
+  ax = fmaf(dx, f, ax);
+  ay = fmaf(dy, f, ay);
+  az = fmaf(dz, f, az);
+}
+
 TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
-                   float rs2, float mass, const float4 *__restrict__ t01, float delta,
-                   float inv_delta, unsigned long long &npp) {
+                   float rs2, const float2 *__restrict__ t0, float wmax, unsigned long long &npp) {
   int lane = threadIdx.x & 31;
   if (lane < m) {
     uint32_t idx = wl.pp[lane];
-    wl.stage[3 * lane + 0] = wrapf(spos[3 * (int64_t)idx + 0], w.rx, cpu);
-    wl.stage[3 * lane + 1] = wrapf(spos[3 * (int64_t)idx + 1], w.ry, cpu);
-    wl.stage[3 * lane + 2] = wrapf(spos[3 * (int64_t)idx + 2], w.rz, cpu);
+    wl.stage[lane] = make_float4(wrapf(spos[3 * (int64_t)idx + 0], w.rx, cpu), wrapf(spos[3 * (int64_t)idx + 1], w.ry, cpu),
+                                 wrapf(spos[3 * (int64_t)idx + 2], w.rz, cpu), 0.f);
   }
   __syncwarp();
-  float ax = 0.f, ay = 0.f, az = 0.f;
-  for (int j = 0; j < m; j++) {
-    float dx = w.tx - wl.stage[3 * j + 0];
-    float dy = w.ty - wl.stage[3 * j + 1];
-    float dz = w.tz - wl.stage[3 * j + 2];
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 <= rs2) {
-      float r = sqrtf(r2);
-      int nt = (int)(r * inv_delta);
-      float t = r - (float)nt * delta;
-      float4 c = t01[nt];
-      float f = (c.x + c.y * t) * mass;
-      ax += dx * f;
-      ay += dy * f;
-      az += dz * f;
-    }
+  float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
+  float a2x = 0.f, a2y = 0.f, a2z = 0.f, a3x = 0.f, a3y = 0.f, a3z = 0.f;
+  int j = 0;
+  for (; j + 4 <= m; j += 4) {
+    pp_body(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
+    pp_body(wl.stage[j + 1], w, rs2, wmax, t0, a1x, a1y, a1z);
+    pp_body(wl.stage[j + 2], w, rs2, wmax, t0, a2x, a2y, a2z);
+    pp_body(wl.stage[j + 3], w, rs2, wmax, t0, a3x, a3y, a3z);
   }
+  for (; j < m; j++) pp_body(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
   if (w.active) {
-    w.ax += ax;
-    w.ay += ay;
-    w.az += az;
+    w.ax += (a0x + a1x) + (a2x + a3x);
+    w.ay += (a0y + a1y) + (a2y + a3y);
+    w.az += (a0z + a1z) + (a2z + a3z);
     npp += (unsigned long long)m;
   }
   __syncwarp();
 }
 
+// Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
+// and z components on their own axes.
+// Coordinates are in table-index units (cells / delta); the quadrupole terms
+// are rescaled to cells with delta before they are added.
 TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, float cpu, float rs2,
-                   const float4 *__restrict__ t01, const float2 *__restrict__ t2, float delta,
-                   float inv_delta, int entries, unsigned long long &npc) {
+                   const float2 *__restrict__ t0, const float4 *__restrict__ t12, float delta,
+                   float wmax, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
   for (int base = 0; base < m_all; base += 32) {
     int m = min(32, m_all - base);
     if (lane < m) {
       uint32_t nd = wl.pc[base + lane];
       float4 m0 = tb.mom0[nd], m1 = tb.mom1[nd], m2 = tb.mom2[nd];
-      float *s = &wl.stage[12 * lane];
-      s[0] = wrapf(__float_as_uint(m0.x), w.rx, cpu);
-      s[1] = wrapf(__float_as_uint(m0.y), w.ry, cpu);
-      s[2] = wrapf(__float_as_uint(m0.z), w.rz, cpu);
-      s[3] = m0.w;
-      s[4] = m1.x;
-      s[5] = m1.y;
-      s[6] = m1.z;
-      s[7] = m1.w;
-      s[8] = m2.x;
-      s[9] = m2.y;
-      s[10] = m2.z;
+      // com in table-index units (cpu here is cells-per-unit / delta)
+      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpu),
+                                           wrapf(__float_as_uint(m0.y), w.ry, cpu),
+                                           wrapf(__float_as_uint(m0.z), w.rz, cpu), m0.w);
+      wl.stage[3 * lane + 1] = m1;  // Qxx Qyy Qzz Qxy
+      wl.stage[3 * lane + 2] = m2;  // Qxz Qyz trQ -
     }
     __syncwarp();
     float ax = 0.f, ay = 0.f, az = 0.f;
     for (int j = 0; j < m; j++) {
-      const float *s = &wl.stage[12 * j];
-      float dx = w.tx - s[0], dy = w.ty - s[1], dz = w.tz - s[2];
-      float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 <= rs2) {
-        float r = sqrtf(r2);
-        int nt = (int)(r * inv_delta);
-        float t = r - (float)nt * delta;
-        nt = min(nt, entries - 1);
-        float4 c = t01[nt];
-        float2 c2 = t2[nt];
-        float f1 = c.x + c.y * t, f2 = c.z + c.w * t, f3 = c2.x + c2.y * t;
-        float Qxx = s[4], Qyy = s[5], Qzz = s[6], Qxy = s[7], Qxz = s[8], Qyz = s[9], trQ = s[10];
-        float q1 = Qxx * dx + Qxy * dy + Qxz * dz;
-        float q2 = Qxy * dx + Qyy * dy + Qyz * dz;
-        float q3 = Qxz * dx + Qyz * dy + Qzz * dz;
-        float qq = Qxx * dx * dx + Qyy * dy * dy + Qzz * dz * dz +
-                   2.f * (Qxy * dx * dy + Qxz * dx * dz + Qyz * dy * dz);
-        float tt = s[3] * f1 + trQ * f2 + qq * f3;
-        float two2 = 2.f * f2;
-        ax += dx * tt + q1 * two2;
-        ay += dy * tt + q2 * two2;
-        az += dz * tt + q3 * two2;
-      }
+      float4 c0 = wl.stage[3 * j], q1 = wl.stage[3 * j + 1], q2 = wl.stage[3 * j + 2];
+      float ux = w.tx - c0.x, uy = w.ty - c0.y, uz = w.tz - c0.z;
+      float r2 = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+      float wq = fminf(r2 * rsqrt_approx(r2), wmax);
+      float dx = ux * delta, dy = uy * delta, dz = uz * delta;
+      float frac;
+      int nt = table_index(wq, frac);
+      float2 c = t0[nt];
+      float4 d = t12[nt];
+      float f1 = fmaf(c.y, frac, c.x), f2 = fmaf(d.y, frac, d.x), f3 = fmaf(d.w, frac, d.z);
+      float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
+      float q1x = Qxx * dx + Qxy * dy + Qxz * dz;
+      float q2y = Qxy * dx + Qyy * dy + Qyz * dz;
+      float q3z = Qxz * dx + Qyz * dy + Qzz * dz;
+      float qq = Qxx * dx * dx + Qyy * dy * dy + Qzz * dz * dz + 2.f * (Qxy * dx * dy + Qxz * dx * dz + Qyz * dy * dz);
+      float tt = c0.w * f1 + trQ * f2 + qq * f3;
+      float two2 = 2.f * f2;
+      bool in = r2 <= rs2;
+      ax += in ? dx * tt + q1x * two2 : 0.f;
+      ay += in ? dy * tt + q2y * two2 : 0.f;
+      az += in ? dz * tt + q3z * two2 : 0.f;
     }
     if (w.active) {
-      w.ax += ax;
-      w.ay += ay;
-      w.az += az;
+      w.bx += ax;
+      w.by += ay;
+      w.bz += az;
       npc += (unsigned long long)m;
     }
     __syncwarp();
   }
 }
 
-__global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
-    const uint32_t *__restrict__ spos, TreeBuffers tb, const float4 *__restrict__ g01,
-    const float2 *__restrict__ g2, int entries, float delta, float inv_delta, float cpu, float rs2,
-    float mass, float *__restrict__ ftree, uint32_t *__restrict__ err) {
+__global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
+    const uint32_t *__restrict__ spos, TreeBuffers tb, const float2 *__restrict__ g0,
+    const float4 *__restrict__ g12, int entries, float inv_delta, float cpu, float rs2, float mass,
+    float *__restrict__ ftree, uint32_t *__restrict__ err) {
+  // positions relative to the group reference in table-index units
+  const float cpi = cpu * inv_delta;
+  const float rs2i = rs2 * inv_delta * inv_delta;
+  const float delta = 1.f / inv_delta;
   extern __shared__ float4 smem4[];
-  float4 *t01 = smem4;
-  float2 *t2 = reinterpret_cast<float2 *>(t01 + entries);
-  WarpLists *lists = reinterpret_cast<WarpLists *>(t2 + entries + (entries & 1));
-  for (int i = threadIdx.x; i < entries; i += kWalkThreads) {
-    t01[i] = g01[i];
-    t2[i] = g2[i];
-  }
+  float4 *t12 = smem4;
+  float2 *t0 = reinterpret_cast<float2 *>(t12 + entries);
+  WarpLists *lists = reinterpret_cast<WarpLists *>(t0 + entries + 1 + ((entries + 1) & 1));
+  for (int i = threadIdx.x; i < entries; i += kWalkThreads) t12[i] = g12[i];
+  for (int i = threadIdx.x; i <= entries; i += kWalkThreads) t0[i] = g0[i];
   __syncthreads();
+  const float wmax = (float)(entries - 1);
   int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpLists &wl = lists[wib];
   int64_t gwarp = (int64_t)blockIdx.x * kWalkWarps + wib;
   uint32_t *stack = tb.stack + gwarp * kStackCap;
   uint32_t ngroups = tb.counters[0];
-  unsigned long long npp = 0, npc = 0;
+  unsigned long long npp = 0, npc = 0, niter = 0, nvisit = 0;
+  int max_top = 0;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
   while (true) {
     uint32_t g = 0;
@@ -599,11 +629,16 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
     w.rx = __shfl_sync(0xffffffffu, ux, 0);
     w.ry = __shfl_sync(0xffffffffu, uy, 0);
     w.rz = __shfl_sync(0xffffffffu, uz, 0);
-    w.tx = w.active ? wrapf(ux, w.rx, cpu) : 0.f;
-    w.ty = w.active ? wrapf(uy, w.ry, cpu) : 0.f;
-    w.tz = w.active ? wrapf(uz, w.rz, cpu) : 0.f;
+    w.tx = w.active ? wrapf(ux, w.rx, cpi) : 0.f;
+    w.ty = w.active ? wrapf(uy, w.ry, cpi) : 0.f;
+    w.tz = w.active ? wrapf(uz, w.rz, cpi) : 0.f;
     w.ax = w.ay = w.az = 0.f;
-    float lox = w.tx, hix = w.tx, loy = w.ty, hiy = w.ty, loz = w.tz, hiz = w.tz;
+    w.bx = w.by = w.bz = 0.f;
+    // group box in cells
+    float gx0 = w.active ? wrapf(ux, w.rx, cpu) : 0.f;
+    float gy0 = w.active ? wrapf(uy, w.ry, cpu) : 0.f;
+    float gz0 = w.active ? wrapf(uz, w.rz, cpu) : 0.f;
+    float lox = gx0, hix = gx0, loy = gy0, hiy = gy0, loz = gz0, hiz = gz0;
     for (int o = 16; o > 0; o >>= 1) {
       lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
       hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
@@ -623,6 +658,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
     bool failed = false;
     while (top > 0) {
       int take = min(top, 32);
+      niter++;
+      nvisit += (unsigned long long)take;
       uint32_t node = 0;
       bool has = lane < take;
       if (has) node = stack[top - take + lane];
@@ -680,20 +717,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
       }
       for (uint32_t j = 0; j < push; j++) stack[top + incl - push + j] = c0 + j;
       top += (int)total;
+      max_top = max(max_top, top);
       __syncwarp();
       // accepted nodes
       unsigned acc = __ballot_sync(0xffffffffu, kind == 1);
       if (acc) {
         int cntv = __popc(acc);
-        if (npcl + cntv > kListCap) {
-          eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
-          npcl = 0;
-        }
         if (kind == 1) wl.pc[npcl + __popc(acc & lanemask_lt)] = node;
         npcl += cntv;
         __syncwarp();
         if (npcl >= 32) {
-          eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
+          eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, t12, delta, wmax, npc);
           npcl = 0;
         }
       }
@@ -713,7 +747,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
           c -= take2;
           __syncwarp();
           if (nppl == 32) {
-            eval_pp(wl, nppl, spos, w, cpu, rs2, mass, t01, delta, inv_delta, npp);
+            eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
             nppl = 0;
           }
         }
@@ -723,13 +757,15 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
       if (lane == 0) atomicOr(err, (uint32_t)kErrStackOverflow);
       continue;
     }
-    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpu, rs2, t01, t2, delta, inv_delta, entries, npc);
-    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpu, rs2, mass, t01, delta, inv_delta, npp);
+    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, t12, delta, wmax, npc);
+    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
     if (w.active) {
+      // the particle sums used separations in index units: back to cells
       int64_t i = (int64_t)gs + lane;
-      ftree[3 * i + 0] = w.ax;
-      ftree[3 * i + 1] = w.ay;
-      ftree[3 * i + 2] = w.az;
+      float md = mass * delta;
+      ftree[3 * i + 0] = fmaf(w.ax, md, w.bx);
+      ftree[3 * i + 1] = fmaf(w.ay, md, w.by);
+      ftree[3 * i + 2] = fmaf(w.az, md, w.bz);
     }
   }
   // interaction counters
@@ -740,6 +776,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_tree_walk(
   if (lane == 0) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[2]), npp);
     atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[4]), npc);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[6]), niter);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[8]), nvisit);
+    atomicMax(&tb.counters[10], (uint32_t)max_top);
   }
 }
 
@@ -764,20 +803,20 @@ int64_t walk_stack_words() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int64_t)sms * 8 * kWalkWarps * kStackCap;
+  return (int64_t)sms * 2 * kWalkWarps * kStackCap;
 }
 
 void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
                const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st, int64_t *launches) {
   (void)np;
-  size_t smem = sizeof(float4) * law.entries + sizeof(float2) * (law.entries + (law.entries & 1)) +
+  size_t smem = sizeof(float4) * law.entries + sizeof(float2) * (law.entries + 1 + ((law.entries + 1) & 1)) +
                 sizeof(WarpLists) * kWalkWarps;
   int grid = walk_grid(smem);
   int64_t max_grid = tb.stack_words / ((int64_t)kWalkWarps * kStackCap);
   if (grid > max_grid) grid = (int)max_grid;
-  k_tree_walk<<<grid, kWalkThreads, smem, st>>>(spos, tb, law.t01, law.t2, law.entries, law.delta,
-                                                law.inv_delta, tp.cell_per_unit,
-                                                tp.rsphere * tp.rsphere, tp.mass, ftree, err);
+  k_tree_walk<<<grid, kWalkThreads, smem, st>>>(spos, tb, law.t0, law.t12, law.entries, law.inv_delta,
+                                                tp.cell_per_unit, tp.rsphere * tp.rsphere, tp.mass, ftree,
+                                                err);
   if (launches) *launches += 1;
 }
 

@@ -271,9 +271,10 @@ class Engine:
         return {STAGES[i]: float(ms[i]) for i in range(k)}
 
     def counters(self) -> dict:
-        c = np.zeros(4, np.int64)
-        self._lib.tpm_counters(self._ctx, c.ctypes.data, 4)
-        return {"nodes": int(c[0]), "pp": int(c[1]), "pc": int(c[2]), "groups": int(c[3])}
+        c = np.zeros(7, np.int64)
+        self._lib.tpm_counters(self._ctx, c.ctypes.data, 7)
+        return {"nodes": int(c[0]), "pp": int(c[1]), "pc": int(c[2]), "groups": int(c[3]),
+                "walk_iterations": int(c[4]), "walk_nodes": int(c[5]), "walk_max_stack": int(c[6])}
 
     def launch_count(self) -> int:
         return int(self._lib.tpm_launch_count(self._ctx))
