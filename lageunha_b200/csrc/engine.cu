@@ -265,7 +265,7 @@ static int alloc_mesh(tpm_ctx *c) {
 static void free_particles(tpm_ctx *c) {
   void *ps[] = {c->pos, c->vel, c->key, c->key_alt, c->val, c->val_alt, c->spos, c->fpm, c->ftree, c->fout,
                 c->ss.hist, c->ss.dtotal, c->tb.start, c->tb.count, c->tb.child, c->tb.nchild, c->tb.level, c->tb.geo,
-                c->tb.mom0, c->tb.mom1, c->tb.mom2, c->tb.tile_sum, c->tb.groups};
+                c->tb.mom0, c->tb.mom1, c->tb.mom2, c->tb.walkA, c->tb.walkB, c->tb.tile_sum, c->tb.groups};
   for (void *p : ps)
     if (p) cudaFree(p);
   c->pos = nullptr;
@@ -280,6 +280,7 @@ static void free_particles(tpm_ctx *c) {
   c->tb.level = nullptr;
   c->tb.geo = nullptr;
   c->tb.mom0 = c->tb.mom1 = c->tb.mom2 = nullptr;
+  c->tb.walkA = c->tb.walkB = nullptr;
   c->tb.tile_sum = nullptr;
   c->tb.groups = nullptr;
   c->cap = 0;
@@ -317,6 +318,8 @@ static int ensure_particles(tpm_ctx *c, int64_t np) {
   CK(cudaMalloc(&tb.mom0, sizeof(float4) * cap_nodes));
   CK(cudaMalloc(&tb.mom1, sizeof(float4) * cap_nodes));
   CK(cudaMalloc(&tb.mom2, sizeof(float4) * cap_nodes));
+  CK(cudaMalloc(&tb.walkA, sizeof(uint4) * 2 * cap_nodes));
+  CK(cudaMalloc(&tb.walkB, sizeof(uint4) * cap_nodes));
   int64_t ts = (cap_nodes + 1023) / 1024 + 16;
   int64_t need_groups = 2 * c->ncubes + (c->ncubes + 4095) / 4096 + 16;
   if (ts < need_groups) ts = need_groups;

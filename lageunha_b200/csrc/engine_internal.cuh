@@ -83,7 +83,12 @@ struct TreeBuffers {
   uint4 *geo = nullptr;      // center u32 x3, half-size (float bits)
   float4 *mom0 = nullptr;    // com (u32 bits x3), mass
   float4 *mom1 = nullptr;    // Qxx Qyy Qzz Qxy
-  float4 *mom2 = nullptr;    // Qxz Qyz trQ open2 (size^2/theta^2)
+  float4 *mom2 = nullptr;    // Qxz Qyz trQ mass
+  // walk records, written with the moments: walkA[2n] = cube centre u32 x3 +
+  // half-size bits, walkA[2n+1] = com u32 x3 + size^2/theta^2 bits;
+  // walkB[n] = start, count, first child, nchild | level << 16
+  uint4 *walkA = nullptr;
+  uint4 *walkB = nullptr;
   uint32_t *level_range = nullptr;  // [2*(kAxisBits+2)] begin/end per level
   uint32_t *tile_sum = nullptr;     // scan scratch
   int64_t cap_tiles = 0;

@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(256) k_tree_moments(const uint32_t *__restrict
       float size = 0.f;
       for (uint32_t j = c0; j < c0 + nch; j++) {
         float4 m0 = tb.mom0[j], m1 = tb.mom1[j], m2 = tb.mom2[j];
+        float child_open2 = __uint_as_float(tb.walkA[2 * (int64_t)j + 1].w);
         float m = m0.w;
         float dx = wrapf(__float_as_uint(m0.x), geo.x, cpu) - cx;
         float dy = wrapf(__float_as_uint(m0.y), geo.y, cpu) - cy;
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(256) k_tree_moments(const uint32_t *__restrict
         qxz += m2.x + m * dx * dz;
         qyz += m2.y + m * dy * dz;
         // child size from its open2 = size^2/theta^2
-        float cs = sqrtf(m2.w / inv_theta2);
+        float cs = sqrtf(child_open2 / inv_theta2);
         size = fmaxf(size, sqrtf(dx * dx + dy * dy + dz * dz) + cs);
       }
       size2 = size * size;
@@ -310,7 +311,11 @@ __global__ void __launch_bounds__(256) k_tree_moments(const uint32_t *__restrict
     uint32_t comz = geo.z + (uint32_t)(int32_t)__float2int_rn(cz / cpu);
     tb.mom0[node] = make_float4(__uint_as_float(comx), __uint_as_float(comy), __uint_as_float(comz), M);
     tb.mom1[node] = make_float4(qxx, qyy, qzz, qxy);
-    tb.mom2[node] = make_float4(qxz, qyz, qxx + qyy + qzz, size2 * inv_theta2);
+    tb.mom2[node] = make_float4(qxz, qyz, qxx + qyy + qzz, M);
+    tb.walkA[2 * (int64_t)node] = geo;
+    tb.walkA[2 * (int64_t)node + 1] = make_uint4(comx, comy, comz, __float_as_uint(size2 * inv_theta2));
+    tb.walkB[node] = make_uint4(tb.start[node], tb.count[node], tb.child[node],
+                                nch | ((uint32_t)tb.level[node] << 16));
   }
 }
 
@@ -450,25 +455,28 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 // ------------------------------------------------------------------ walk
 constexpr int kWalkWarps = 16;
 constexpr int kWalkThreads = kWalkWarps * 32;
-constexpr int kStackCap = 8192;
-constexpr int kListCap = 64;
+constexpr int kStackSmem = 640;    // per-warp stack entries in shared memory
+constexpr int kStackCap = 8192;    // entries beyond kStackSmem live in global memory
+constexpr int kPcCap = 64;
+constexpr int kPpBatch = 96;       // particle sources evaluated per flush
 
 struct WarpLists {
-  uint32_t pc[kListCap];
-  uint32_t pp[kListCap];
-  float4 stage[32 * 3];  // PP: one float4 per source; PC: three per node
+  uint32_t pc[kPcCap];
+  uint32_t pp[kPpBatch];
+  float4 stage[kPpBatch];          // PP: one float4 per source; PC: three per node
+  uint32_t stack[kStackSmem];
 };
 
 struct WalkCtx {
-  float tx, ty, tz;       // this lane's target relative to u_ref
-  float ax, ay, az;       // particle-particle sum (without the particle mass)
-  float bx, by, bz;       // particle-node sum
+  float tx, ty, tz;       // this lane's target relative to u_ref (table-index units)
+  float ax, ay, az;       // particle-particle sum (index units, without the particle mass)
+  float bx, by, bz;       // particle-node sum (cells)
   bool active;
   uint32_t rx, ry, rz;    // u_ref
 };
 
 // Hardware reciprocal square root (MUFU), flushing denormals: the walk's
-// distances are at least 2^-32 cells apart or exactly zero.
+// separations are at least 2^-32 cells apart or exactly zero.
 TPM_D float rsqrt_approx(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -505,13 +513,26 @@ TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, cons
   az = fmaf(dz, f, az);
 }
 
-TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
+TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpi,
                    float rs2, const float2 *__restrict__ t0, float wmax, unsigned long long &npp) {
   int lane = threadIdx.x & 31;
-  if (lane < m) {
-    uint32_t idx = wl.pp[lane];
-    wl.stage[lane] = make_float4(wrapf(spos[3 * (int64_t)idx + 0], w.rx, cpu), wrapf(spos[3 * (int64_t)idx + 1], w.ry, cpu),
-                                 wrapf(spos[3 * (int64_t)idx + 2], w.rz, cpu), 0.f);
+  // all loads of the batch are issued before any is used
+  uint32_t u[kPpBatch / 32][3];
+#pragma unroll
+  for (int b = 0; b < kPpBatch / 32; b++) {
+    int k = b * 32 + lane;
+    if (k < m) {
+      uint32_t idx = wl.pp[k];
+      u[b][0] = spos[3 * (int64_t)idx + 0];
+      u[b][1] = spos[3 * (int64_t)idx + 1];
+      u[b][2] = spos[3 * (int64_t)idx + 2];
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < kPpBatch / 32; b++) {
+    int k = b * 32 + lane;
+    if (k < m)
+      wl.stage[k] = make_float4(wrapf(u[b][0], w.rx, cpi), wrapf(u[b][1], w.ry, cpi), wrapf(u[b][2], w.rz, cpi), 0.f);
   }
   __syncwarp();
   float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
@@ -534,10 +555,9 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 }
 
 // Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
-// and z components on their own axes.
-// Coordinates are in table-index units (cells / delta); the quadrupole terms
-// are rescaled to cells with delta before they are added.
-TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, float cpu, float rs2,
+// and z components on their own axes. Coordinates are in table-index units;
+// the separations are rescaled to cells with delta for the force terms.
+TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, float cpi, float rs2,
                    const float2 *__restrict__ t0, const float4 *__restrict__ t12, float delta,
                    float wmax, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
@@ -546,12 +566,11 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, 
     if (lane < m) {
       uint32_t nd = wl.pc[base + lane];
       float4 m0 = tb.mom0[nd], m1 = tb.mom1[nd], m2 = tb.mom2[nd];
-      // com in table-index units (cpu here is cells-per-unit / delta)
-      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpu),
-                                           wrapf(__float_as_uint(m0.y), w.ry, cpu),
-                                           wrapf(__float_as_uint(m0.z), w.rz, cpu), m0.w);
+      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpi),
+                                           wrapf(__float_as_uint(m0.y), w.ry, cpi),
+                                           wrapf(__float_as_uint(m0.z), w.rz, cpi), m0.w);
       wl.stage[3 * lane + 1] = m1;  // Qxx Qyy Qzz Qxy
-      wl.stage[3 * lane + 2] = m2;  // Qxz Qyz trQ -
+      wl.stage[3 * lane + 2] = m2;  // Qxz Qyz trQ mass
     }
     __syncwarp();
     float ax = 0.f, ay = 0.f, az = 0.f;
@@ -564,7 +583,7 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, 
       float frac;
       int nt = table_index(wq, frac);
       float2 c = t0[nt];
-      float4 d = t12[nt];
+      float4 d = __ldg(&t12[nt]);
       float f1 = fmaf(c.y, frac, c.x), f2 = fmaf(d.y, frac, d.x), f3 = fmaf(d.w, frac, d.z);
       float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
       float q1x = Qxx * dx + Qxy * dy + Qxz * dz;
@@ -588,6 +607,20 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, 
   }
 }
 
+// The walk stack: the first kStackSmem entries in shared memory, the rest in
+// this warp's global region.
+struct WarpStack {
+  uint32_t *sm;
+  uint32_t *gl;
+  TPM_D uint32_t get(int i) const { return i < kStackSmem ? sm[i] : gl[i - kStackSmem]; }
+  TPM_D void put(int i, uint32_t v) {
+    if (i < kStackSmem)
+      sm[i] = v;
+    else
+      gl[i - kStackSmem] = v;
+  }
+};
+
 __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     const uint32_t *__restrict__ spos, TreeBuffers tb, const float2 *__restrict__ g0,
     const float4 *__restrict__ g12, int entries, float inv_delta, float cpu, float rs2, float mass,
@@ -597,17 +630,15 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
   const float rs2i = rs2 * inv_delta * inv_delta;
   const float delta = 1.f / inv_delta;
   extern __shared__ float4 smem4[];
-  float4 *t12 = smem4;
-  float2 *t0 = reinterpret_cast<float2 *>(t12 + entries);
-  WarpLists *lists = reinterpret_cast<WarpLists *>(t0 + entries + 1 + ((entries + 1) & 1));
-  for (int i = threadIdx.x; i < entries; i += kWalkThreads) t12[i] = g12[i];
+  float2 *t0 = reinterpret_cast<float2 *>(smem4);
+  WarpLists *lists = reinterpret_cast<WarpLists *>(smem4 + (entries + 2) / 2);
   for (int i = threadIdx.x; i <= entries; i += kWalkThreads) t0[i] = g0[i];
   __syncthreads();
   const float wmax = (float)(entries - 1);
   int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpLists &wl = lists[wib];
   int64_t gwarp = (int64_t)blockIdx.x * kWalkWarps + wib;
-  uint32_t *stack = tb.stack + gwarp * kStackCap;
+  WarpStack stack{wl.stack, tb.stack + gwarp * (kStackCap - kStackSmem)};
   uint32_t ngroups = tb.counters[0];
   unsigned long long npp = 0, npc = 0, niter = 0, nvisit = 0;
   int max_top = 0;
@@ -652,53 +683,53 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     // a little slack against float rounding of the relative coordinates
     float rs2_prune = rs2 * 1.0001f + 1e-4f;
     int top = 0, npcl = 0, nppl = 0;
-    if (lane == 0) stack[0] = 0;
+    if (lane == 0) stack.put(0, 0u);
     top = 1;
     __syncwarp();
     bool failed = false;
     while (top > 0) {
-      int take = min(top, 32);
+      // narrower pops keep a deep frontier from growing further
+      int take = min(top, top > kStackSmem / 2 ? 8 : 32);
       niter++;
       nvisit += (unsigned long long)take;
       uint32_t node = 0;
       bool has = lane < take;
-      if (has) node = stack[top - take + lane];
+      if (has) node = stack.get(top - take + lane);
       __syncwarp();
       top -= take;
-      // classify
+      // classify: one 32-byte and one 16-byte record per node
       int kind = 0;  // 0 drop, 1 accept (PC), 2 open (push children), 3 particles (PP)
       uint32_t c0 = 0, nch = 0, ps = 0, pcnt = 0;
       if (has) {
-        uint4 geo = tb.geo[node];
-        int lev = tb.level[node];
+        uint4 geo = tb.walkA[2 * (int64_t)node];
+        uint4 com = tb.walkA[2 * (int64_t)node + 1];
+        uint4 rec = tb.walkB[node];
+        int lev = (int)(rec.w >> 16);
+        nch = rec.w & 0xffffu;
         float half = __uint_as_float(geo.w);
         float dx = fmaxf(fabsf(wrapf(geo.x, w.rx, cpu) - cx) - half - hx, 0.f);
         float dy = fmaxf(fabsf(wrapf(geo.y, w.ry, cpu) - cy) - half - hy, 0.f);
         float dz = fmaxf(fabsf(wrapf(geo.z, w.rz, cpu) - cz) - half - hz, 0.f);
         bool near = lev < 2 || dx * dx + dy * dy + dz * dz <= rs2_prune;
         if (near) {
-          uint32_t cnt = tb.count[node];
-          nch = tb.nchild[node];
-          if (lev > 0 && cnt < (uint32_t)kLeafMin) {
+          if (lev > 0 && rec.y < (uint32_t)kLeafMin) {
             kind = 3;
-            ps = tb.start[node];
-            pcnt = cnt;
+            ps = rec.x;
+            pcnt = rec.y;
           } else {
-            float4 m0 = tb.mom0[node];
-            float open2 = tb.mom2[node].w;
-            float ex = fmaxf(fabsf(wrapf(__float_as_uint(m0.x), w.rx, cpu) - cx) - hx, 0.f);
-            float ey = fmaxf(fabsf(wrapf(__float_as_uint(m0.y), w.ry, cpu) - cy) - hy, 0.f);
-            float ez = fmaxf(fabsf(wrapf(__float_as_uint(m0.z), w.rz, cpu) - cz) - hz, 0.f);
-            bool open = lev < 2 || ex * ex + ey * ey + ez * ez < open2;
+            float ex = fmaxf(fabsf(wrapf(com.x, w.rx, cpu) - cx) - hx, 0.f);
+            float ey = fmaxf(fabsf(wrapf(com.y, w.ry, cpu) - cy) - hy, 0.f);
+            float ez = fmaxf(fabsf(wrapf(com.z, w.rz, cpu) - cz) - hz, 0.f);
+            bool open = lev < 2 || ex * ex + ey * ey + ez * ez < __uint_as_float(com.w);
             if (!open)
               kind = 1;
             else if (nch > 0) {
               kind = 2;
-              c0 = tb.child[node];
+              c0 = rec.z;
             } else {
               kind = 3;
-              ps = tb.start[node];
-              pcnt = cnt;
+              ps = rec.x;
+              pcnt = rec.y;
             }
           }
         }
@@ -715,7 +746,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         failed = true;
         break;
       }
-      for (uint32_t j = 0; j < push; j++) stack[top + incl - push + j] = c0 + j;
+      for (uint32_t j = 0; j < push; j++) stack.put(top + (int)(incl - push + j), c0 + j);
       top += (int)total;
       max_top = max(max_top, top);
       __syncwarp();
@@ -727,7 +758,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         npcl += cntv;
         __syncwarp();
         if (npcl >= 32) {
-          eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, t12, delta, wmax, npc);
+          eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, g12, delta, wmax, npc);
           npcl = 0;
         }
       }
@@ -739,14 +770,14 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         uint32_t s = __shfl_sync(0xffffffffu, ps, src);
         uint32_t c = __shfl_sync(0xffffffffu, pcnt, src);
         while (c > 0) {
-          uint32_t room = (uint32_t)(32 - nppl);
-          uint32_t take2 = min(room, c);
+          uint32_t room = (uint32_t)(kPpBatch - nppl);
+          uint32_t take2 = min(min(room, c), 32u);
           if ((uint32_t)lane < take2) wl.pp[nppl + lane] = s + lane;
           nppl += (int)take2;
           s += take2;
           c -= take2;
           __syncwarp();
-          if (nppl == 32) {
+          if (nppl == kPpBatch) {
             eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
             nppl = 0;
           }
@@ -757,7 +788,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
       if (lane == 0) atomicOr(err, (uint32_t)kErrStackOverflow);
       continue;
     }
-    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, t12, delta, wmax, npc);
+    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, g12, delta, wmax, npc);
     if (nppl > 0) eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
     if (w.active) {
       // the particle sums used separations in index units: back to cells
@@ -772,12 +803,14 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
   for (int o = 16; o > 0; o >>= 1) {
     npp += __shfl_down_sync(0xffffffffu, npp, o);
     npc += __shfl_down_sync(0xffffffffu, npc, o);
+    niter += __shfl_down_sync(0xffffffffu, niter, o);
+    nvisit += __shfl_down_sync(0xffffffffu, nvisit, o);
   }
   if (lane == 0) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[2]), npp);
     atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[4]), npc);
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[6]), niter);
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[8]), nvisit);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[6]), niter / 32);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[8]), nvisit / 32);
     atomicMax(&tb.counters[10], (uint32_t)max_top);
   }
 }
@@ -803,16 +836,15 @@ int64_t walk_stack_words() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int64_t)sms * 2 * kWalkWarps * kStackCap;
+  return (int64_t)sms * 2 * kWalkWarps * (kStackCap - kStackSmem);
 }
 
 void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
                const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st, int64_t *launches) {
   (void)np;
-  size_t smem = sizeof(float4) * law.entries + sizeof(float2) * (law.entries + 1 + ((law.entries + 1) & 1)) +
-                sizeof(WarpLists) * kWalkWarps;
+  size_t smem = sizeof(float4) * ((law.entries + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
   int grid = walk_grid(smem);
-  int64_t max_grid = tb.stack_words / ((int64_t)kWalkWarps * kStackCap);
+  int64_t max_grid = tb.stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
   if (grid > max_grid) grid = (int)max_grid;
   k_tree_walk<<<grid, kWalkThreads, smem, st>>>(spos, tb, law.t0, law.t12, law.entries, law.inv_delta,
                                                 tp.cell_per_unit, tp.rsphere * tp.rsphere, tp.mass, ftree,
