@@ -79,7 +79,7 @@ def _displacement_field(n: int, rng: np.random.Generator, spec_index: float, dam
     dk = wk * amp
     psi = np.empty((3, n, n, n), dtype=np.float64)
     for c, kc in enumerate((kx, ky, kz)):
-        psi[c] = np.fft.irfftn(1j * kc * dk / k2, s=(n, n, n))
+        psi[c] = np.fft.irfftn(1j * kc * dk / k2, s=(n, n, n), axes=(0, 1, 2))
     rms = np.sqrt(np.mean(np.sum(psi * psi, axis=0)))
     psi *= rms_target / rms
     return psi
