@@ -184,6 +184,33 @@ int tpm_read_order(tpm_ctx *ctx, uint64_t *keys, uint32_t *perm);
 #define TPM_MESH_POTENTIAL 1
 int tpm_read_mesh(tpm_ctx *ctx, int which, float *out);
 
+/* ---- allocation-free ordering ---- */
+
+/* Largest particle count tpm_morton_order_noalloc accepts: its scratch is a
+ * fixed array of about 3.1 MB compiled into the library. */
+#define TPM_NOALLOC_MAX_PARTICLES 262144
+
+/* No counterpart in the reference. The engine's Morton ordering (the keys
+ * and stable radix sort of tpm_compute_forces, bit-identical results) for
+ * callers that cannot allocate device memory: codes that run all of the GPU's
+ * memory through their own pool, where a library cudaMalloc would fail or
+ * escape the pool's accounting, and latency-critical loops that cannot take
+ * the device-wide synchronisation of cudaMalloc/cudaFree. It allocates
+ * nothing: its scratch is a fixed device array of the library, reserved on
+ * every GPU that loads it until the process exits.
+ *   pos   device pointer, np x 3 uint32 fixed-point positions (AoS)
+ *   keys  device pointer, np uint64: sorted 39-bit Morton keys (output)
+ *   perm  device pointer, np uint32: sorted slot -> input index (output)
+ *   stream  a cudaStream_t (NULL: the legacy default stream)
+ * Work is queued on `stream`; the call does not wait for it. np above
+ * TPM_NOALLOC_MAX_PARTICLES is rejected with TPM_E_ARG. The first call on a
+ * device looks up the device address of its scratch (cudaGetSymbolAddress,
+ * with that device current), so make that first call before any stream
+ * capture. All calls share the one scratch array: calls whose work overlaps
+ * on the GPU race and must be serialised by the caller. */
+int tpm_morton_order_noalloc(const uint32_t *pos, int64_t np, int32_t n_mesh, uint64_t *keys,
+                             uint32_t *perm, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,8 @@ static bool debug_sync() {
   return v == 1;
 }
 
+void tpm::set_last_error(const char *msg) { g_err = msg; }
+
 static int fail(int code, const char *fmt, ...) {
   char buf[512];
   va_list ap;

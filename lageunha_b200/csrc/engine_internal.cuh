@@ -128,6 +128,9 @@ void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const Tre
                int64_t *launches);
 
 // ---------------------------------------------------------------- misc
+// Sets the message tpm_last_error() returns on this thread.
+void set_last_error(const char *msg);
+
 void launch_finish_forces(const uint32_t *perm, int64_t np, const float *fpm, const float *ftree,
                           unsigned parts, float *force_out, cudaStream_t st);
 

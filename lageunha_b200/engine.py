@@ -83,6 +83,7 @@ _SIGS = {
     "tpm_launch_count": (_I64, [_P]),
     "tpm_read_order": (ctypes.c_int, [_P, _P, _P]),
     "tpm_read_mesh": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "tpm_morton_order_noalloc": (ctypes.c_int, [_P, _I64, ctypes.c_int32, _P, _P, _P]),
 }
 
 
