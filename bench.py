@@ -2,12 +2,19 @@
 """TreePM force-evaluation benchmark.
 
 One step = one full TreePM force evaluation (Morton sort, TSC deposit,
-Poisson FFT, fda4 gradient + interpolation, tree build, tree walk, forces
+Poisson FFT, gradient + interpolation, tree build, tree walk, forces
 scattered back to the caller's order) of the clustered 256^3 workload:
 256^3 particles on a 256^3 mesh, L = 200 Mpc/h, Zel'dovich field with
 P(k) ~ k^-2 exp(-(0.5k)^2) and 1.5-spacing rms displacement plus 200 Plummer
 spheres (a = 0.64 cells, 2000-20000 particles each), softening 0.05 cells,
-theta 0.3, rsphere 4, efold 0.9 (the reference's law).
+theta 0.3.
+
+The metric is quoted at rms force error <= 1e-3 against the FP64 Ewald sum.
+The reference's own split law (PMFITPARA residual, efold 0.9, rsphere 4)
+stays near 3.5e-3 on this workload, so the headline uses the engine's
+Gaussian split (rs = 1.2 cells, short-range cut at 6 cells, 8-point
+gradient), which measures rms ~6e-4; the same line also carries the
+reference law's throughput and error ("reference_law").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -36,6 +43,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Mparticles/s per TreePM force eval (plain vs batched) at rms err≤1e-3; p50/p99 latency"
 UNIT = "Mparticles/s"
 EPS = 0.05
+HEADLINE_LAW = {"law": "gaussian", "rs_split": 1.2, "rsphere": 6.0, "theta": 0.3, "efold": 0.9}
+REFERENCE_LAW = {"law": "reference", "rs_split": 1.25, "rsphere": 4.0, "theta": 0.3, "efold": 0.9}
 FP32_LANES_PER_SM = 128
 # FLOPs charged per evaluated interaction of the walk (DESIGN.md derives them):
 # particle-particle 20, particle-node (quadrupole) 65
@@ -207,7 +216,8 @@ def run_engine_arm(args):
     pu = ps.positions_u32()
     npart = ps.np
 
-    eng = E.Engine(n, epsilon=EPS, theta=0.3, rsphere=4.0, efold=0.9, device=local)
+    law = REFERENCE_LAW if args.law == "reference" else HEADLINE_LAW
+    eng = E.Engine(n, epsilon=EPS, device=local, **law)
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
     pos_dev = torch.from_numpy(pu.view(np.int32)).to(f"cuda:{local}")
     f_dev = torch.empty((npart, 3), dtype=torch.float32, device=f"cuda:{local}")
@@ -299,6 +309,27 @@ def run_engine_arm(args):
     clocks = _clock_summary(clk_path, local)
     peaks = _peaks()
 
+    # ---- the reference's law in the same run (the drop-in parity mode)
+    ref_law = None
+    if args.law != "reference" and not args.no_reference_law:
+        eng.set_params(law="reference", rsphere=REFERENCE_LAW["rsphere"])
+        for _ in range(2):
+            step_dev()
+        barrier()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        for _ in range(args.steps):
+            step_dev()
+        r1.record(stream)
+        barrier()
+        ms_ref = r0.elapsed_time(r1) / args.steps
+        ref_law = {"value": ws * npart / (ms_ref * 1e-3) / 1e6, "ms_per_step": ms_ref, **REFERENCE_LAW}
+        if err is not None:
+            fr = f_dev.cpu().numpy()
+            e = np.linalg.norm(fr[tg].astype(np.float64) - few, axis=1) / np.linalg.norm(few, axis=1)
+            ref_law["err_vs_ewald"] = {"rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99))}
+
     # ---- roofline of the dominant kernel
     per = {k: v / args.steps for k, v in stages.items()}
     dominant = max(per, key=per.get)
@@ -335,8 +366,7 @@ def run_engine_arm(args):
         "data": "synthetic (seeded Zel'dovich field + Plummer spheres; no dataset)",
         "config": {"workload": args.workload + (f" at {n}^3" if args.scale else "") +
                                " (one TreePM force evaluation per step, plain engine)",
-                   "n_mesh": n, "particles_per_gpu": npart, "theta": 0.3, "rsphere": 4.0, "epsilon": EPS,
-                   "efold": 0.9, "law": "reference",
+                   "n_mesh": n, "particles_per_gpu": npart, "epsilon": EPS, **law,
                    "l2": f"inputs larger than L2: {12 * npart / 1e6:.0f} MB of positions, "
                          f"{4 * n ** 3 / 1e6:.0f} MB mesh",
                    "parallelism": f"replicas x{ws}"},
@@ -345,6 +375,7 @@ def run_engine_arm(args):
         "hbm_stages": hbm_stages,
         "counters": counters,
         "err_vs_ewald": err,
+        "reference_law": ref_law,
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 12 * npart,
                 "d2h_bytes_per_step": 12 * npart},
@@ -372,6 +403,9 @@ def main():
     ap.add_argument("--workload", default="clustered256", choices=["clustered256", "plain64", "scale512"])
     ap.add_argument("--scale", type=int, default=None,
                     help="mesh size of a smaller instance of the workload (profiling captures)")
+    ap.add_argument("--law", default="gaussian", choices=["gaussian", "reference"],
+                    help="force law of the headline (gaussian: rms <= 1e-3 vs Ewald)")
+    ap.add_argument("--no-reference-law", action="store_true")
     ap.add_argument("--no-ewald", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -88,7 +88,7 @@ struct tpm_ctx {
   float *rho = nullptr;
   float2 *spec = nullptr;
   float *phi = nullptr;
-  CUtensorMap tmap;
+  CUtensorMap tmap2, tmap4;  // potential boxes for the 4- and 8-point gradients
   uint32_t *tile_start = nullptr;
   // tree
   TreeBuffers tb;
@@ -256,7 +256,8 @@ static int alloc_mesh(tpm_ctx *c) {
   c->ncubes = 1ll << (3 * (g.cbits - 2));
   CK(cudaMalloc(&c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
   fft_plan_init(c->fp, g.n);
-  if (make_phi_tensor_map(g, c->phi, &c->tmap) != 0) return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
+  if (make_phi_tensor_map(g, c->phi, 2, &c->tmap2) != 0 || make_phi_tensor_map(g, c->phi, 4, &c->tmap4) != 0)
+    return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
   CK(cudaGetLastError());
   // set-up work above ran on the legacy stream; the context stream is
   // non-blocking, so finish it before any force evaluation
@@ -604,7 +605,12 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st, &c->launches);
     CK(stage_check(st, "fft"));
     CK(cudaEventRecord(c->ev[3], st));
-    launch_fda4(g, &c->tmap, c->phi, c->spos, c->tile_start, c->fpm, c->err, st);
+    // the reference law keeps the reference's 4-point gradient; the Gaussian
+    // law uses the 8-point one
+    if (c->prm.law == TPM_LAW_REFERENCE)
+      launch_fda4(g, &c->tmap2, 2, c->spos, c->tile_start, c->fpm, c->err, st);
+    else
+      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, st);
     c->launches += 1;
     CK(stage_check(st, "fda4"));
     CK(cudaEventRecord(c->ev[4], st));

@@ -52,7 +52,7 @@ struct MeshGeom {
   int px, py, pz; // ghosted potential pitches (x padded to a multiple of 4)
 };
 constexpr int kTile = 8;     // PM tile: 8^3 cells
-constexpr int kGhost = 4;    // ghost layers of the padded potential
+constexpr int kGhost = 8;    // ghost layers of the padded potential (8-point stencil + TSC)
 
 MeshGeom make_geom(int n);
 
@@ -70,10 +70,11 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
                     int64_t *launches);
 // fda4: gradient and TSC interpolation per tile through TMA.
-void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, const float *phi_pad,
-                 const uint32_t *spos, const uint32_t *tile_start, float *fpm, uint32_t *err,
-                 cudaStream_t st);
-int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out);
+void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
+                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st);
+// Tensor maps of the potential for the 4-point (radius 2) and the 8-point
+// (radius 4) gradient: their boxes differ.
+int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorMap *out);
 
 // ---------------------------------------------------------------- tree
 struct TreeBuffers {

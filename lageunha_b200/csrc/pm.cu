@@ -642,9 +642,21 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
 }
 
 // ------------------------------------------------------------------ fda4
-constexpr int kBoxX = 16, kBoxY = kTile + 7, kBoxZ = kTile + 7;  // phi tile + halo
-constexpr int kNodes = kTile + 3;                                 // gradient nodes per axis
+// Per 8^3 tile: one TMA load of the potential around the tile, the gradient
+// -dphi/dx at the (T+3)^3 TSC nodes in shared memory, then each particle sums
+// its 27 nodes with the TSC weights in the reference's order.
+//   radius 2: the reference's 4-point stencil, 2/3 and -1/12 (fda4.c:45-46)
+//   radius 4: the 8-point stencil 4/5, -1/5, 4/105, -1/280 (the Gaussian law)
+constexpr int kNodes = kTile + 3;  // gradient nodes per axis
 constexpr int kFdaThreads = 256;
+
+template <int R>
+struct FdaBox {
+  static constexpr int H = R + 1;                   // node halo + stencil
+  static constexpr int X0 = ((H + 3) / 4) * 4;      // x starts at t - X0 (16-byte aligned)
+  static constexpr int BX = ((X0 + kTile + H + 3) / 4) * 4;
+  static constexpr int BY = kTile + 2 * H + 1;
+};
 
 TPM_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -664,14 +676,20 @@ TPM_D bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int64_t limit) {
   return false;
 }
 
+template <int R>
 __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CUtensorMap tmap,
                                                       const uint32_t *__restrict__ spos,
                                                       const uint32_t *__restrict__ tile_start, int n,
                                                       int cbits, float *__restrict__ fpm,
                                                       uint32_t *__restrict__ err) {
-  __shared__ __align__(128) float box[kBoxZ][kBoxY][kBoxX];
-  __shared__ float gx[kNodes * kNodes * kNodes], gy[kNodes * kNodes * kNodes],
-      gz[kNodes * kNodes * kNodes];
+  using B = FdaBox<R>;
+  // dynamic shared memory: the potential box (128-byte aligned for TMA), then
+  // the three gradient components
+  extern __shared__ __align__(128) float fda_smem[];
+  float(*box)[B::BY][B::BX] = reinterpret_cast<float(*)[B::BY][B::BX]>(fda_smem);
+  float *gx = fda_smem + B::BY * B::BY * B::BX;
+  float *gy = gx + kNodes * kNodes * kNodes;
+  float *gz = gy + kNodes * kNodes * kNodes;
   __shared__ __align__(8) uint64_t bar;
   int tid = threadIdx.x;
   uint32_t t = blockIdx.x;
@@ -692,10 +710,10 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
   __syncthreads();
   if (tid == 0) {
     uint32_t a = smem_u32(&bar);
-    uint32_t bytes = sizeof(box);
+    uint32_t bytes = sizeof(float) * B::BY * B::BY * B::BX;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
-    // box origin in padded coordinates: x from x0-4 (aligned), y,z from -3
-    int cx = x0 - 4 + kGhost, cy = y0 - 3 + kGhost, cz = z0 - 3 + kGhost;
+    // box origin in padded coordinates: x from x0 - X0 (aligned), y,z from -H
+    int cx = x0 - B::X0 + kGhost, cy = y0 - B::H + kGhost, cz = z0 - B::H + kGhost;
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(&box[0][0][0])),
@@ -707,16 +725,30 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
     mbar_wait_bounded(&bar, 0, 1ll << 20);  // let an in-flight copy land before exit
     return;
   }
-  // gradient at nodes [t-1, t+T+1]^3: -dphi/dx with the 4-point stencil
-  const float ff1 = (4.f / 3.f) / 2.f, ff2 = (-1.f / 3.f) / 4.f;
+  // gradient at nodes [t-1, t+T+1]^3
   for (int i = tid; i < kNodes * kNodes * kNodes; i += kFdaThreads) {
     int a = i % kNodes, r = i / kNodes;
     int b = r % kNodes, c = r / kNodes;
-    // node (x0-1+a, y0-1+b, z0-1+c) -> box (a+3, b+2, c+2)
-    int bx = a + 3, by = b + 2, bz = c + 2;
-    gx[i] = ff1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + ff2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]);
-    gy[i] = ff1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + ff2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]);
-    gz[i] = ff1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + ff2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]);
+    // node (x0-1+a, y0-1+b, z0-1+c) -> box (a-1+X0, b-1+H, c-1+H)
+    int bx = a - 1 + B::X0, by = b - 1 + B::H, bz = c - 1 + B::H;
+    float fx, fy, fz;
+    if (R == 2) {
+      const float f1 = (4.f / 3.f) / 2.f, f2 = (-1.f / 3.f) / 4.f;
+      fx = f1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + f2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]);
+      fy = f1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + f2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]);
+      fz = f1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + f2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]);
+    } else {
+      const float c1 = 4.f / 5.f, c2 = -1.f / 5.f, c3 = 4.f / 105.f, c4 = -1.f / 280.f;
+      fx = c1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + c2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]) +
+           c3 * (box[bz][by][bx - 3] - box[bz][by][bx + 3]) + c4 * (box[bz][by][bx - 4] - box[bz][by][bx + 4]);
+      fy = c1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + c2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]) +
+           c3 * (box[bz][by - 3][bx] - box[bz][by + 3][bx]) + c4 * (box[bz][by - 4][bx] - box[bz][by + 4][bx]);
+      fz = c1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + c2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]) +
+           c3 * (box[bz - 3][by][bx] - box[bz + 3][by][bx]) + c4 * (box[bz - 4][by][bx] - box[bz + 4][by][bx]);
+    }
+    gx[i] = fx;
+    gy[i] = fy;
+    gz[i] = fz;
   }
   __syncthreads();
   uint32_t nu = (uint32_t)n;
@@ -738,8 +770,7 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
     for (int c = 0; c < 3; c++)
 #pragma unroll
       for (int b = 0; b < 3; b++) {
-        float wxy0 = wxs[0] * wys[b], wxy1 = wxs[1] * wys[b], wxy2 = wxs[2] * wys[b];
-        float wab[3] = {wxy0, wxy1, wxy2};
+        float wab[3] = {wxs[0] * wys[b], wxs[1] * wys[b], wxs[2] * wys[b]};
 #pragma unroll
         for (int a = 0; a < 3; a++) {
           float wt = wab[a] * wzs[c];
@@ -760,7 +791,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out) {
+int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorMap *out) {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
@@ -772,7 +803,14 @@ int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out) {
   }
   cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
   cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.py * 4};
-  cuuint32_t box[3] = {kBoxX, kBoxY, kBoxZ};
+  cuuint32_t box[3];
+  if (radius == 2) {
+    box[0] = FdaBox<2>::BX;
+    box[1] = box[2] = FdaBox<2>::BY;
+  } else {
+    box[0] = FdaBox<4>::BX;
+    box[1] = box[2] = FdaBox<4>::BY;
+  }
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, phi_pad, dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -780,12 +818,19 @@ int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, CUtensorMap *out) {
   return r == CUDA_SUCCESS ? 0 : -2;
 }
 
-void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, const float *phi_pad,
-                 const uint32_t *spos, const uint32_t *tile_start, float *fpm, uint32_t *err,
-                 cudaStream_t st) {
-  (void)phi_pad;
+void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
+                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st) {
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
-  k_fda4<<<ntiles, kFdaThreads, 0, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+  const size_t nodes = sizeof(float) * 3 * kNodes * kNodes * kNodes;
+  if (radius == 2) {
+    size_t smem = sizeof(float) * FdaBox<2>::BY * FdaBox<2>::BY * FdaBox<2>::BX + nodes;
+    cudaFuncSetAttribute(k_fda4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fda4<2><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+  } else {
+    size_t smem = sizeof(float) * FdaBox<4>::BY * FdaBox<4>::BY * FdaBox<4>::BX + nodes;
+    cudaFuncSetAttribute(k_fda4<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fda4<4><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+  }
 }
 
 }  // namespace tpm
