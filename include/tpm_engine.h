@@ -151,6 +151,63 @@ int tpm_treecorrection(tpm_ctx *ctx, void *treedm_particles, int64_t np, float f
  * (Treemain.c:598-601) and stays set on the context, then treecorrection. */
 int tpm_treemain(tpm_ctx *ctx, void *treedm_particles, int64_t np, float fact2, int stepcount);
 
+/* ---- the global step (expanding background) ---- */
+
+/* Cosmology of the background: OMEP, OMEPLAM, WLAM0, WLAM1 and AMAX of the
+ * reference's SimParameters (eunha.h:1056-1072). */
+typedef struct tpm_cosmology {
+  float omep, omeplam, wlam0, wlam1, amax;
+} tpm_cosmology;
+
+/* The reference's EvolFact (Cosmos/CosmosEvolFactor.h:1-6); afact and bfact
+ * are unused and set to 0. */
+typedef struct tpm_evolfact {
+  float afact, bfact, pfact;
+  float fact1, fact2;
+  float fact1_push, fact2_push;
+  float fact1_pull, fact2_pull;
+} tpm_evolfact;
+
+/* GetEvolFactor (Cosmos/CosmosEvolFactor.c:230-255) for the step from
+ * anow - astep/2 to anow + astep/2 on an nx^3 mesh; host only, no GPU. */
+int tpm_evol_factors(const tpm_cosmology *cosmo, int32_t nx, float anow, float astep, tpm_evolfact *out);
+
+/* v *= fact1 (HubbleDragDM, Cosmos/globalT.c:102-110). */
+int tpm_hubble_drag(tpm_ctx *ctx, float fact1);
+
+/* One GOTPM global step in KICK status (Cosmos/globalT.c:221-305 between
+ * synchronisation points): Hubble drag with fact1, PM and tree kicks with
+ * fact2, drift with pfact = astep * NX. With the reference law the opening
+ * angle follows TreeAndPreFoFmain's step schedule (Cosmos/globalT.c:41-44).
+ * The caller advances anow by astep afterwards. */
+int tpm_step(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t stepcount);
+
+/* ---- captured evaluations and ensembles ---- */
+
+/* tpm_compute_forces replayed from a CUDA graph captured on the first call
+ * (and again whenever the particle count, buffers or parameters change): the
+ * same kernels and results, one launch, no stage times or counters. No
+ * counterpart in the reference, which evaluates one box per process. */
+int tpm_graph_compute(tpm_ctx *ctx, unsigned parts);
+
+/* An ensemble of independent boxes (contexts on one device, each with its own
+ * particle count, mesh size and parameters). One call evaluates every box
+ * through one graph launch built from the boxes' captured graphs, so their
+ * kernels overlap on the device, and synchronises once. The boxes stay owned
+ * by the caller and must outlive the batch. No counterpart in the reference
+ * (one box per MPI job). */
+typedef struct tpm_batch tpm_batch;
+int tpm_batch_create(tpm_ctx *const *boxes, int32_t nbox, tpm_batch **out);
+int tpm_batch_destroy(tpm_batch *batch);
+/* Forces of `parts` in every box, as tpm_compute_forces per box. */
+int tpm_batch_compute(tpm_batch *batch, unsigned parts);
+/* One global step per box (drag, forces, kicks, drift, as tpm_step without
+ * the opening-angle schedule), box i at expansion factor anow[i] with step
+ * astep[i]. */
+int tpm_batch_step(tpm_batch *batch, const tpm_cosmology *cosmo, const float *anow, const float *astep);
+/* Device time of the last tpm_batch_compute / tpm_batch_step launch, ms. */
+int tpm_batch_time(tpm_batch *batch, float *ms);
+
 /* ---- diagnostics ---- */
 
 /* FP64 periodic Ewald force (reference units, Plummer softening epsilon on

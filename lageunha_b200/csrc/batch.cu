@@ -1,0 +1,227 @@
+// Captured force evaluations and ensembles of boxes.
+//
+// A context's force evaluation (or its whole global step) is captured once
+// into a CUDA graph and replayed while its buffers and parameters stay the
+// same (tpm_ctx::gen and np). The step graph reads its evolution factors from
+// device words that a copy node at its head fills from pinned host memory, so
+// one graph serves every step. Error words travel back through a copy node
+// at its tail.
+//
+// An ensemble (tpm_batch) puts the graphs of all its boxes side by side as
+// child nodes of one graph: one launch evaluates every box, the boxes'
+// kernels overlap on the device, and the host waits once. Boxes of different
+// particle counts and mesh sizes mix freely; each keeps its own device state
+// between launches.
+#include <string.h>
+
+#include <vector>
+
+#include "ctx.cuh"
+
+using namespace tpm;
+
+namespace {
+
+void drop_graph(CapturedGraph &gr) {
+  if (gr.exec) cudaGraphExecDestroy(gr.exec);
+  if (gr.graph) cudaGraphDestroy(gr.graph);
+  gr.exec = nullptr;
+  gr.graph = nullptr;
+  gr.gen = 0;
+  gr.np = -1;
+}
+
+int capture_body(tpm_ctx *c, int kind) {
+  cudaStream_t st = c->st;
+  if (kind == kGraphStep) {
+    CK(cudaMemcpyAsync(c->dfac, c->hfac, sizeof(double) * kFacWords, cudaMemcpyHostToDevice, st));
+    int rc = launch_drag(c, st, 1.f, c->dfac);
+    if (!rc) rc = enqueue_forces(c, TPM_PART_ALL, st, false);
+    if (!rc) rc = launch_kick(c, st, 0.f, 0.f, c->dfac);
+    if (!rc) rc = launch_drift(c, st, 0.0, c->dfac);
+    if (rc) return rc;
+  } else {
+    int rc = enqueue_forces(c, (unsigned)kind, st, false);
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(c->herr, c->err, sizeof(uint32_t) * 8, cudaMemcpyDeviceToHost, st));
+  return 0;
+}
+
+}  // namespace
+
+int tpm::ensure_graph(tpm_ctx *c, int kind) {
+  CapturedGraph &gr = c->graphs[kind];
+  if (gr.exec && gr.gen == c->gen && gr.np == c->np) return 0;
+  drop_graph(gr);
+  CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+  int rc = capture_body(c, kind);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->st, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(TPM_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&gr.exec, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return fail(TPM_E_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+  }
+  gr.graph = g;
+  gr.gen = c->gen;
+  gr.np = c->np;
+  return 0;
+}
+
+// ------------------------------------------------------------------ ensembles
+struct tpm_batch {
+  std::vector<tpm_ctx *> boxes;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  // the ensemble graph per kind, with the box graphs' (gen, np) it was built on
+  cudaGraphExec_t exec[kNGraphs] = {};
+  std::vector<uint64_t> sig_gen[kNGraphs];
+  std::vector<int64_t> sig_np[kNGraphs];
+  float last_ms = 0.f;
+};
+
+namespace {
+
+int ensure_batch_graph(tpm_batch *b, int kind) {
+  bool fresh = b->exec[kind] != nullptr;
+  for (size_t i = 0; i < b->boxes.size() && fresh; i++) {
+    const CapturedGraph &gr = b->boxes[i]->graphs[kind];
+    fresh = gr.exec && gr.gen == b->sig_gen[kind][i] && gr.np == b->sig_np[kind][i] &&
+            gr.gen == b->boxes[i]->gen && gr.np == b->boxes[i]->np;
+  }
+  if (fresh) return 0;
+  for (tpm_ctx *c : b->boxes) {
+    int rc = ensure_graph(c, kind);
+    if (rc) return rc;
+  }
+  if (b->exec[kind]) cudaGraphExecDestroy(b->exec[kind]);
+  b->exec[kind] = nullptr;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  for (tpm_ctx *c : b->boxes) {
+    cudaGraphNode_t node;
+    cudaError_t e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, c->graphs[kind].graph);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return fail(TPM_E_CUDA, "cudaGraphAddChildGraphNode: %s", cudaGetErrorString(e));
+    }
+  }
+  cudaError_t e = cudaGraphInstantiate(&b->exec[kind], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(TPM_E_CUDA, "ensemble graph instantiation failed: %s", cudaGetErrorString(e));
+  b->sig_gen[kind].resize(b->boxes.size());
+  b->sig_np[kind].resize(b->boxes.size());
+  for (size_t i = 0; i < b->boxes.size(); i++) {
+    b->sig_gen[kind][i] = b->boxes[i]->gen;
+    b->sig_np[kind][i] = b->boxes[i]->np;
+  }
+  return 0;
+}
+
+int run_batch(tpm_batch *b, int kind) {
+  CK(cudaSetDevice(b->device));
+  for (tpm_ctx *c : b->boxes)
+    if (c->np <= 0) return fail(TPM_E_STATE, "a box of the ensemble has no particles");
+  int rc = ensure_batch_graph(b, kind);
+  if (rc) return rc;
+  // work queued on the boxes' own streams comes first
+  for (tpm_ctx *c : b->boxes) CK(cudaStreamSynchronize(c->st));
+  CK(cudaEventRecord(b->t0, b->st));
+  CK(cudaGraphLaunch(b->exec[kind], b->st));
+  CK(cudaEventRecord(b->t1, b->st));
+  CK(cudaEventSynchronize(b->t1));
+  CK(cudaEventElapsedTime(&b->last_ms, b->t0, b->t1));
+  unsigned parts = kind == kGraphStep ? 0u : (unsigned)kind;
+  int first = 0;
+  for (tpm_ctx *c : b->boxes) {
+    int r = finish_forces(c, kind == kGraphStep ? TPM_PART_ALL : parts, true, false);
+    if (kind == kGraphStep) c->parts_valid = 0;  // the drift moved the particles
+    if (r && !first) first = r;
+  }
+  return first;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpm_batch_create(tpm_ctx *const *boxes, int32_t nbox, tpm_batch **out) {
+  if (!out || !boxes || nbox <= 0) return fail(TPM_E_ARG, "bad arguments to tpm_batch_create");
+  *out = nullptr;
+  for (int i = 0; i < nbox; i++) {
+    if (!boxes[i]) return fail(TPM_E_ARG, "box %d is NULL", i);
+    if (boxes[i]->device != boxes[0]->device) return fail(TPM_E_ARG, "boxes on different devices");
+    for (int j = 0; j < i; j++)
+      if (boxes[j] == boxes[i]) return fail(TPM_E_ARG, "box %d repeated", i);
+  }
+  tpm_batch *b = new tpm_batch();
+  b->boxes.assign(boxes, boxes + nbox);
+  b->device = boxes[0]->device;
+  cudaSetDevice(b->device);
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->t0) != cudaSuccess || cudaEventCreate(&b->t1) != cudaSuccess) {
+    tpm_batch_destroy(b);
+    return fail(TPM_E_CUDA, "stream/event creation failed");
+  }
+  *out = b;
+  return 0;
+}
+
+int tpm_batch_destroy(tpm_batch *b) {
+  if (!b) return 0;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (cudaGraphExec_t &x : b->exec)
+    if (x) cudaGraphExecDestroy(x);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return 0;
+}
+
+int tpm_batch_compute(tpm_batch *b, unsigned parts) {
+  if (!b) return fail(TPM_E_ARG, "batch is NULL");
+  parts &= TPM_PART_ALL;
+  if (!parts) return fail(TPM_E_ARG, "no force part requested");
+  return run_batch(b, (int)parts);
+}
+
+int tpm_batch_step(tpm_batch *b, const tpm_cosmology *cosmo, const float *anow, const float *astep) {
+  if (!b || !cosmo || !anow || !astep) return fail(TPM_E_ARG, "bad arguments to tpm_batch_step");
+  // the previous launch has finished (run_batch waits), so the pinned factor
+  // words are free to change
+  for (size_t i = 0; i < b->boxes.size(); i++) {
+    int rc = step_factors(b->boxes[i], cosmo, anow[i], astep[i], b->boxes[i]->hfac);
+    if (rc) return rc;
+  }
+  return run_batch(b, kGraphStep);
+}
+
+int tpm_batch_time(tpm_batch *b, float *ms) {
+  if (!b || !ms) return fail(TPM_E_ARG, "NULL argument");
+  *ms = b->last_ms;
+  return 0;
+}
+
+int tpm_graph_compute(tpm_ctx *c, unsigned parts) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  parts &= TPM_PART_ALL;
+  if (!parts) return fail(TPM_E_ARG, "no force part requested");
+  CK(cudaSetDevice(c->device));
+  int rc = ensure_graph(c, (int)parts);
+  if (rc) return rc;
+  CK(cudaGraphLaunch(c->graphs[parts].exec, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return finish_forces(c, parts, true, false);
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// The engine context (one periodic box on one GPU) shared by the translation
+// units that drive it: engine.cu (the plain C ABI), step.cu (the global step),
+// batch.cu (captured graphs, ensembles) and server.cu (the request loop).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "engine_internal.cuh"
+#include "tpm_engine.h"
+
+namespace tpm {
+
+enum Stage { kStSort = 0, kStDeposit, kStFft, kStFda4, kStTreeBuild, kStTreeWalk, kStFinish, kNStages };
+
+// Graphs a context keeps: one force evaluation per part mask (1..3) and one
+// global step (drag, forces, kick, drift), each valid for the buffers and
+// parameters it was captured with.
+enum GraphKind { kGraphPm = 1, kGraphTree = 2, kGraphAll = 3, kGraphStep = 4, kNGraphs = 5 };
+
+struct CapturedGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t gen = 0;
+  int64_t np = -1;
+};
+
+// Per-box evolution factors as the step graph reads them:
+// [0] fact1 (drag), [1] fact2 (kicks), [2] pfact (drift), [3] unused.
+constexpr int kFacWords = 4;
+
+}  // namespace tpm
+
+struct tpm_ctx {
+  tpm_params prm;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[tpm::kNStages + 1];
+  // particles
+  int64_t np = 0, cap = 0;
+  uint32_t *pos = nullptr;
+  float *vel = nullptr;
+  uint64_t *key = nullptr, *key_alt = nullptr;
+  uint32_t *val = nullptr, *val_alt = nullptr;
+  uint32_t *perm = nullptr;  // sorted -> caller index (one of val/val_alt)
+  uint64_t *skey = nullptr;  // sorted keys (one of key/key_alt)
+  uint32_t *spos = nullptr;
+  float *fpm = nullptr, *ftree = nullptr;  // sorted order
+  float *fout = nullptr;                   // caller order scratch
+  void *stage = nullptr;                   // record staging for the Lagrangian layout
+  size_t stage_bytes = 0;
+  tpm::SortScratch ss;
+  // mesh
+  tpm::MeshGeom g;
+  tpm::FftPlan fp;
+  float *rho = nullptr;
+  float2 *spec = nullptr;
+  float *phi = nullptr;
+  CUtensorMap tmap2, tmap4;  // potential boxes for the 4- and 8-point gradients
+  uint32_t *tile_start = nullptr;
+  // tree
+  tpm::TreeBuffers tb;
+  uint32_t *cube_start = nullptr;
+  int64_t ncubes = 0;
+  tpm::LawTable law;
+  int law_n = -1;
+  float law_eps = -1, law_rs = -1, law_rsphere = -1;
+  int law_kind = -1;
+  uint32_t *err = nullptr;
+  // graphs: gen counts every change of buffers or parameters baked into a
+  // captured launch; herr/hfac are pinned host words the graphs copy through
+  uint64_t gen = 1;
+  tpm::CapturedGraph graphs[tpm::kNGraphs];
+  uint32_t *herr = nullptr;  // pinned [8]
+  double *hfac = nullptr;    // pinned [kFacWords]
+  double *dfac = nullptr;    // device [kFacWords]
+  // bookkeeping
+  unsigned parts_valid = 0;
+  float stage_ms[tpm::kNStages];
+  int64_t launches = 0;
+  int64_t counters[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace tpm {
+
+// Sets the thread's error message and returns code.
+int fail(int code, const char *fmt, ...);
+const std::string &last_error_string();
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess)                                                                            \
+      return ::tpm::fail(e_ == cudaErrorMemoryAllocation ? TPM_E_NOMEM : TPM_E_CUDA, "%s: %s (%s:%d)", \
+                         #call, cudaGetErrorString(e_), __FILE__, __LINE__);                          \
+  } while (0)
+
+// Enqueues one force evaluation of the loaded particles on st (no host
+// synchronisation); with timing, records the stage events.
+int enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing);
+// After the stream has finished an evaluation: checks the device error words
+// (from c->err, or from the pinned copy when from_host), and on success marks
+// the parts valid and reads the tree counters.
+int finish_forces(tpm_ctx *c, unsigned parts, bool from_host, bool timing);
+// v *= fact1; v += fact2 F; x += v pfact. With fac != nullptr the factors are
+// read on the device from fac[0..2] (the step graph); else the scalars apply.
+int launch_drag(tpm_ctx *c, cudaStream_t st, float fact1, const double *fac);
+int launch_kick(tpm_ctx *c, cudaStream_t st, float f2pm, float f2tree, const double *fac);
+int launch_drift(tpm_ctx *c, cudaStream_t st, double pfact, const double *fac);
+// The reference's opening-angle schedule (Cosmos/globalT.c:41-44).
+float theta_schedule(int stepcount);
+// Makes c->graphs[kind] current (captures it again after a change).
+int ensure_graph(tpm_ctx *c, int kind);
+// Host-side evolution factors of one step (fact1, fact2, pfact).
+int step_factors(const tpm_ctx *c, const tpm_cosmology *cosmo, float anow, float astep, double fac[kFacWords]);
+
+}  // namespace tpm

@@ -11,6 +11,7 @@
 
 #include "tpm_engine.h"
 #include "engine_internal.cuh"
+#include "ctx.cuh"
 
 namespace tpm {
 int ewald_force(const uint32_t *pos, int64_t np, int n, float eps, int64_t nt, const int64_t *targets_host,
@@ -35,7 +36,7 @@ static bool debug_sync() {
 
 void tpm::set_last_error(const char *msg) { g_err = msg; }
 
-static int fail(int code, const char *fmt, ...) {
+int tpm::fail(int code, const char *fmt, ...) {
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -45,67 +46,17 @@ static int fail(int code, const char *fmt, ...) {
   return code;
 }
 
-#define CK(call)                                                                        \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess)                                                              \
-      return fail(e_ == cudaErrorMemoryAllocation ? TPM_E_NOMEM : TPM_E_CUDA, "%s: %s (%s:%d)", #call, \
-                  cudaGetErrorString(e_), __FILE__, __LINE__);                          \
-  } while (0)
+const std::string &tpm::last_error_string() { return g_err; }
 
 static cudaError_t stage_check(cudaStream_t st, const char *name) {
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess && debug_sync()) e = cudaStreamSynchronize(st);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (e == cudaSuccess && debug_sync() && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+      cs == cudaStreamCaptureStatusNone)
+    e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) fprintf(stderr, "tpm: stage %s failed: %s\n", name, cudaGetErrorString(e));
   return e;
 }
-
-enum Stage { kStSort = 0, kStDeposit, kStFft, kStFda4, kStTreeBuild, kStTreeWalk, kStFinish, kNStages };
-
-struct tpm_ctx {
-  tpm_params prm;
-  int device = 0;
-  cudaStream_t st = nullptr;
-  cudaEvent_t ev[kNStages + 1];
-  bool timing = true;
-  // particles
-  int64_t np = 0, cap = 0;
-  uint32_t *pos = nullptr;
-  float *vel = nullptr;
-  uint64_t *key = nullptr, *key_alt = nullptr;
-  uint32_t *val = nullptr, *val_alt = nullptr;
-  uint32_t *perm = nullptr;  // sorted -> caller index (one of val/val_alt)
-  uint64_t *skey = nullptr;  // sorted keys (one of key/key_alt)
-  uint32_t *spos = nullptr;
-  float *fpm = nullptr, *ftree = nullptr;  // sorted order
-  float *fout = nullptr;                   // caller order scratch
-  void *stage = nullptr;                   // record staging for the Lagrangian layout
-  size_t stage_bytes = 0;
-  SortScratch ss;
-  // mesh
-  MeshGeom g;
-  FftPlan fp;
-  float *rho = nullptr;
-  float2 *spec = nullptr;
-  float *phi = nullptr;
-  CUtensorMap tmap2, tmap4;  // potential boxes for the 4- and 8-point gradients
-  uint32_t *tile_start = nullptr;
-  // tree
-  TreeBuffers tb;
-  uint32_t *cube_start = nullptr;
-  int64_t ncubes = 0;
-  LawTable law;
-  int law_n = -1;
-  float law_eps = -1, law_rs = -1, law_rsphere = -1;
-  int law_kind = -1;
-  uint32_t *err = nullptr;
-  // bookkeeping
-  unsigned parts_valid = 0;
-  float stage_ms[kNStages];
-  unsigned stage_mask = 0;
-  int64_t launches = 0;
-  int64_t counters[7] = {0, 0, 0, 0, 0, 0, 0};
-};
 
 extern "C" {
 
@@ -208,6 +159,7 @@ static int build_law(tpm_ctx *c) {
                          (float)(slope[3 * i + 2] * dl));
   }
   t0[entries] = make_float2(0.f, 0.f);
+  if (c->law.t0 || c->law.t12) CK(cudaStreamSynchronize(c->st));
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
   c->law.t0 = nullptr;
@@ -224,6 +176,7 @@ static int build_law(tpm_ctx *c) {
   c->law_kind = p.law;
   c->law_rs = p.rs_split;
   c->law_rsphere = p.rsphere;
+  c->gen++;
   return 0;
 }
 
@@ -243,6 +196,8 @@ static void free_mesh(tpm_ctx *c) {
 }
 
 static int alloc_mesh(tpm_ctx *c) {
+  // buffers about to be freed may still be read by queued work
+  CK(cudaStreamSynchronize(c->st));
   free_mesh(c);
   c->g = make_geom(c->prm.n_mesh);
   const MeshGeom &g = c->g;
@@ -250,18 +205,17 @@ static int alloc_mesh(tpm_ctx *c) {
   CK(cudaMalloc(&c->rho, sizeof(float) * n3));
   CK(cudaMalloc(&c->spec, sizeof(float2) * g.spec_elems));
   CK(cudaMalloc(&c->phi, sizeof(float) * (int64_t)g.px * g.py * g.pz));
-  CK(cudaMemset(c->phi, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  CK(cudaMemsetAsync(c->phi, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz, c->st));
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
   CK(cudaMalloc(&c->tile_start, sizeof(uint32_t) * (ntiles + 1)));
   c->ncubes = 1ll << (3 * (g.cbits - 2));
   CK(cudaMalloc(&c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
-  fft_plan_init(c->fp, g.n);
+  fft_plan_init(c->fp, g.n, c->st);
   if (make_phi_tensor_map(g, c->phi, 2, &c->tmap2) != 0 || make_phi_tensor_map(g, c->phi, 4, &c->tmap4) != 0)
     return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
   CK(cudaGetLastError());
-  // set-up work above ran on the legacy stream; the context stream is
-  // non-blocking, so finish it before any force evaluation
-  CK(cudaDeviceSynchronize());
+  // the set-up kernels ran on the context stream, ahead of any evaluation
+  c->gen++;
   return 0;
 }
 
@@ -291,7 +245,9 @@ static void free_particles(tpm_ctx *c) {
 
 static int ensure_particles(tpm_ctx *c, int64_t np) {
   if (np <= c->cap) return 0;
+  CK(cudaStreamSynchronize(c->st));
   free_particles(c);
+  c->gen++;
   int64_t cap = np;
   CK(cudaMalloc(&c->pos, sizeof(uint32_t) * 3 * cap));
   CK(cudaMalloc(&c->vel, sizeof(float) * 3 * cap));
@@ -392,8 +348,17 @@ __global__ void k_finish(const uint32_t *__restrict__ perm, int64_t np, const fl
   }
 }
 
+// v += fact2_pm F_pm + fact2_tree F_tree, in the caller's particle order. The
+// step graph passes fac (fac[1] = fact2 for both parts, each part applied if
+// it was evaluated).
 __global__ void k_kick(const uint32_t *__restrict__ perm, int64_t np, const float *__restrict__ fpm,
-                       const float *__restrict__ ftree, float f2pm, float f2tree, float *__restrict__ vel) {
+                       const float *__restrict__ ftree, float f2pm, float f2tree, float *__restrict__ vel,
+                       const double *__restrict__ fac, unsigned parts) {
+  if (fac) {
+    float f2 = (float)fac[1];
+    f2pm = (parts & TPM_PART_PM) ? f2 : 0.f;
+    f2tree = (parts & TPM_PART_TREE) ? f2 : 0.f;
+  }
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
     int64_t j = perm[i];
     for (int a = 0; a < 3; a++) {
@@ -407,13 +372,21 @@ __global__ void k_kick(const uint32_t *__restrict__ perm, int64_t np, const floa
 
 // x += v * pfact (cells) in FP64, onto the exact periodic fixed point.
 __global__ void k_drift(uint32_t *__restrict__ pos, const float *__restrict__ vel, int64_t np, double pfact,
-                        double units_per_cell) {
+                        double units_per_cell, const double *__restrict__ fac) {
+  if (fac) pfact = fac[2];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 3 * np; i += (int64_t)gridDim.x * blockDim.x) {
     double d = (double)vel[i] * pfact * units_per_cell;
     double m = fmod(d, 4294967296.0);
     long long s = llrint(m);
     pos[i] = pos[i] + (uint32_t)(unsigned long long)s;
   }
+}
+
+// Hubble drag v *= fact1 (HubbleDragDM, Cosmos/globalT.c:102-110).
+__global__ void k_drag(float *__restrict__ vel, int64_t n3, float f, const double *__restrict__ fac) {
+  if (fac) f = (float)fac[0];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
+    vel[i] *= f;
 }
 
 int grid_for(int64_t n, int threads = 256) {
@@ -424,6 +397,26 @@ int grid_for(int64_t n, int threads = 256) {
 }
 
 }  // namespace
+
+int tpm::launch_drag(tpm_ctx *c, cudaStream_t st, float fact1, const double *fac) {
+  k_drag<<<grid_for(3 * c->np), 256, 0, st>>>(c->vel, 3 * c->np, fact1, fac);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int tpm::launch_kick(tpm_ctx *c, cudaStream_t st, float f2pm, float f2tree, const double *fac) {
+  k_kick<<<grid_for(c->np), 256, 0, st>>>(c->perm, c->np, c->fpm, c->ftree, f2pm, f2tree, c->vel, fac,
+                                          TPM_PART_ALL);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int tpm::launch_drift(tpm_ctx *c, cudaStream_t st, double pfact, const double *fac) {
+  double upc = 4294967296.0 / (double)c->prm.n_mesh;
+  k_drift<<<grid_for(3 * c->np), 256, 0, st>>>(c->pos, c->vel, c->np, pfact, upc, fac);
+  CK(cudaGetLastError());
+  return 0;
+}
 
 extern "C" {
 
@@ -459,7 +452,15 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
     tpm_destroy(c);
     return fail(TPM_E_NOMEM, "cudaMalloc of walk stacks failed");
   }
-  cudaMemset(c->err, 0, sizeof(uint32_t) * 8);
+  if (cudaMallocHost(&c->herr, sizeof(uint32_t) * 8) != cudaSuccess ||
+      cudaMallocHost(&c->hfac, sizeof(double) * kFacWords) != cudaSuccess ||
+      cudaMalloc(&c->dfac, sizeof(double) * kFacWords) != cudaSuccess) {
+    tpm_destroy(c);
+    return fail(TPM_E_NOMEM, "allocation of step scratch failed");
+  }
+  memset(c->herr, 0, sizeof(uint32_t) * 8);
+  memset(c->hfac, 0, sizeof(double) * kFacWords);
+  cudaMemsetAsync(c->err, 0, sizeof(uint32_t) * 8, c->st);
   rc = alloc_mesh(c);
   if (!rc) rc = build_law(c);
   if (rc) {
@@ -484,6 +485,13 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->tb.level_range) cudaFree(c->tb.level_range);
   if (c->tb.stack) cudaFree(c->tb.stack);
   if (c->stage) cudaFree(c->stage);
+  for (CapturedGraph &gr : c->graphs) {
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    if (gr.graph) cudaGraphDestroy(gr.graph);
+  }
+  if (c->herr) cudaFreeHost(c->herr);
+  if (c->hfac) cudaFreeHost(c->hfac);
+  if (c->dfac) cudaFree(c->dfac);
   for (int i = 0; i <= kNStages; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->st) cudaStreamDestroy(c->st);
@@ -497,6 +505,7 @@ int tpm_set_params(tpm_ctx *c, const tpm_params *p) {
   if (rc) return rc;
   CK(cudaSetDevice(c->device));
   bool remesh = p->n_mesh != c->prm.n_mesh;
+  if (memcmp(p, &c->prm, sizeof(*p)) != 0) c->gen++;
   c->prm = *p;
   if (remesh) {
     CK(cudaStreamSynchronize(c->st));
@@ -569,17 +578,14 @@ int tpm_load_lagrangian(tpm_ctx *c, int64_t np, const void *particles, int64_t s
   return 0;
 }
 
-int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
-  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
-  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
-  if ((parts & TPM_PART_ALL) == 0) return fail(TPM_E_ARG, "no force part requested");
-  CK(cudaSetDevice(c->device));
+}  // extern "C"
+
+int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing) {
   const MeshGeom &g = c->g;
-  cudaStream_t st = c->st;
   int64_t np = c->np;
   c->launches = 0;
   CK(cudaMemsetAsync(c->err, 0, sizeof(uint32_t) * 8, st));
-  CK(cudaEventRecord(c->ev[0], st));
+  if (timing) CK(cudaEventRecord(c->ev[0], st));
   // ---- sort
   launch_make_keys(c->pos, np, (uint32_t)g.n, g.sub_bits, c->key, c->val, st);
   uint64_t *k = c->key;
@@ -592,7 +598,7 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
   launch_gather_pos(c->pos, c->perm, np, c->spos, st);
   c->launches += 2;
   CK(stage_check(st, "sort"));
-  CK(cudaEventRecord(c->ev[1], st));
+  if (timing) CK(cudaEventRecord(c->ev[1], st));
   // ---- PM
   if (parts & TPM_PART_PM) {
     uint32_t ntiles = 1u << (3 * (g.cbits - 3));
@@ -601,10 +607,10 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st);
     c->launches += 2;
     CK(stage_check(st, "deposit"));
-    CK(cudaEventRecord(c->ev[2], st));
+    if (timing) CK(cudaEventRecord(c->ev[2], st));
     launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st, &c->launches);
     CK(stage_check(st, "fft"));
-    CK(cudaEventRecord(c->ev[3], st));
+    if (timing) CK(cudaEventRecord(c->ev[3], st));
     // the reference law keeps the reference's 4-point gradient; the Gaussian
     // law uses the 8-point one
     if (c->prm.law == TPM_LAW_REFERENCE)
@@ -613,8 +619,8 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
       launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, st);
     c->launches += 1;
     CK(stage_check(st, "fda4"));
-    CK(cudaEventRecord(c->ev[4], st));
-  } else {
+    if (timing) CK(cudaEventRecord(c->ev[4], st));
+  } else if (timing) {
     for (int i = 2; i <= 4; i++) CK(cudaEventRecord(c->ev[i], st));
   }
   // ---- tree
@@ -630,18 +636,26 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     CK(cudaMemsetAsync(c->tb.counters, 0, sizeof(uint32_t) * 16, st));
     tree_groups(tp, c->skey, np, c->tb, c->cube_start, c->ncubes, 3 * (g.sub_bits + 2), st, &c->launches);
     CK(stage_check(st, "tree_build"));
-    CK(cudaEventRecord(c->ev[5], st));
+    if (timing) CK(cudaEventRecord(c->ev[5], st));
     tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
     CK(stage_check(st, "tree_walk"));
-    CK(cudaEventRecord(c->ev[6], st));
-  } else {
+    if (timing) CK(cudaEventRecord(c->ev[6], st));
+  } else if (timing) {
     for (int i = 5; i <= 6; i++) CK(cudaEventRecord(c->ev[i], st));
   }
-  CK(cudaEventRecord(c->ev[7], st));
+  if (timing) CK(cudaEventRecord(c->ev[7], st));
   CK(cudaGetLastError());
+  return 0;
+}
+
+int tpm::finish_forces(tpm_ctx *c, unsigned parts, bool from_host, bool timing) {
   uint32_t herr[8];
-  CK(cudaMemcpyAsync(herr, c->err, sizeof(herr), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  if (from_host) {
+    memcpy(herr, c->herr, sizeof(herr));
+  } else {
+    CK(cudaMemcpyAsync(herr, c->err, sizeof(herr), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
   if (herr[0]) {
     c->parts_valid = 0;
     if (herr[0] & kErrNodeOverflow) return fail(TPM_E_OVERFLOW, "tree node capacity exceeded");
@@ -649,17 +663,17 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
     if (herr[0] & kErrTmaTimeout) return fail(TPM_E_CUDA, "TMA load timed out in fda4");
     return fail(TPM_E_CUDA, "device error flags 0x%x", herr[0]);
   }
-  for (int s = 0; s < kNStages; s++) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev[s], c->ev[s + 1]);
-    c->stage_ms[s] = ms;
-  }
-  // counters: nodes, pp, pc, groups
-  {
+  if (timing) {
+    for (int s = 0; s < kNStages; s++) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev[s], c->ev[s + 1]);
+      c->stage_ms[s] = ms;
+    }
+    // counters: nodes, pp, pc, groups
     uint32_t hc[12];
     uint32_t lr[2 * (kAxisBits + 2)];
-    cudaMemcpy(hc, c->tb.counters, sizeof(hc), cudaMemcpyDeviceToHost);
-    cudaMemcpy(lr, c->tb.level_range, sizeof(lr), cudaMemcpyDeviceToHost);
+    CK(cudaMemcpy(hc, c->tb.counters, sizeof(hc), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(lr, c->tb.level_range, sizeof(lr), cudaMemcpyDeviceToHost));
     uint32_t nn = 0;
     for (int l = 0; l <= kAxisBits; l++)
       if (lr[2 * l + 1] > nn) nn = lr[2 * l + 1];
@@ -673,6 +687,18 @@ int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
   }
   c->parts_valid = parts & TPM_PART_ALL;
   return 0;
+}
+
+extern "C" {
+
+int tpm_compute_forces(tpm_ctx *c, unsigned parts) {
+  if (!c) return fail(TPM_E_ARG, "ctx is NULL");
+  if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
+  if ((parts & TPM_PART_ALL) == 0) return fail(TPM_E_ARG, "no force part requested");
+  CK(cudaSetDevice(c->device));
+  int rc = enqueue_forces(c, parts, c->st, true);
+  if (rc) return rc;
+  return finish_forces(c, parts, false, true);
 }
 
 int tpm_read_forces(tpm_ctx *c, float *out, int mem) {
@@ -692,20 +718,16 @@ int tpm_kick(tpm_ctx *c, float fact2_pm, float fact2_tree) {
   if (!(c->parts_valid & TPM_PART_PM)) fact2_pm = 0.f;
   if (!(c->parts_valid & TPM_PART_TREE)) fact2_tree = 0.f;
   CK(cudaSetDevice(c->device));
-  k_kick<<<grid_for(c->np), 256, 0, c->st>>>(c->perm, c->np, c->fpm, c->ftree, fact2_pm, fact2_tree, c->vel);
-  CK(cudaGetLastError());
-  return 0;
+  return launch_kick(c, c->st, fact2_pm, fact2_tree, nullptr);
 }
 
 int tpm_drift(tpm_ctx *c, double pfact) {
   if (!c) return fail(TPM_E_ARG, "ctx is NULL");
   if (c->np <= 0) return fail(TPM_E_STATE, "no particles loaded");
   CK(cudaSetDevice(c->device));
-  double upc = 4294967296.0 / (double)c->prm.n_mesh;
-  k_drift<<<grid_for(3 * c->np), 256, 0, c->st>>>(c->pos, c->vel, c->np, pfact, upc);
-  CK(cudaGetLastError());
+  int rc = launch_drift(c, c->st, pfact, nullptr);
   c->parts_valid = 0;
-  return 0;
+  return rc;
 }
 
 int tpm_read_velocities(tpm_ctx *c, float *out, int mem) {
@@ -784,7 +806,7 @@ int tpm_treemain(tpm_ctx *c, void *tdm, int64_t np, float fact2, int stepcount) 
   if (!c) return fail(TPM_E_ARG, "ctx is NULL");
   tpm_params p = c->prm;
   // Treemain.c:598-601
-  p.theta = stepcount < 10 ? 0.3f : (stepcount < 20 ? 0.35f : (stepcount < 60 ? 0.4f : 0.45f));
+  p.theta = theta_schedule(stepcount);
   int rc = tpm_set_params(c, &p);
   if (!rc) rc = tpm_treecorrection(c, tdm, np, fact2);
   return rc;

@@ -64,7 +64,8 @@ struct FftPlan {
   float2 *tw_half = nullptr;
   int n = 0;
 };
-void fft_plan_init(FftPlan &p, int n);
+// twiddle tables are written on st
+void fft_plan_init(FftPlan &p, int n, cudaStream_t st);
 void fft_plan_free(FftPlan &p);
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,

@@ -386,17 +386,17 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
 __global__ void k_fft_cols(float2 *__restrict__ spec, struct FftArgs a, const float2 *__restrict__ tw_n, int axis,
                            float dir, int with_green, struct GreenArgs ga, int TX);
 
-void fft_plan_init(FftPlan &p, int n) {
+void fft_plan_init(FftPlan &p, int n, cudaStream_t st) {
   p.n = n;
   const int max_smem = 160 * 1024;
   cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   cudaMalloc(&p.tw, sizeof(float2) * n);
-  k_twiddles<<<(n + 255) / 256, 256>>>(p.tw, n);
+  k_twiddles<<<(n + 255) / 256, 256, 0, st>>>(p.tw, n);
   int h = n / 2 > 0 ? n / 2 : 1;
   cudaMalloc(&p.tw_half, sizeof(float2) * h);
-  k_twiddles<<<(h + 255) / 256, 256>>>(p.tw_half, h);
+  k_twiddles<<<(h + 255) / 256, 256, 0, st>>>(p.tw_half, h);
 }
 
 void fft_plan_free(FftPlan &p) {

@@ -816,19 +816,22 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
 }
 
 static int walk_grid(size_t smem) {
-  static int cached = 0;
-  static size_t cached_smem = 0;
-  if (cached && cached_smem == smem) return cached;
-  cudaFuncSetAttribute(k_tree_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // The dynamic shared-memory cap is raised once to the largest table a law
+  // can have (4096 + 1 entries), so graphs captured for contexts with
+  // different tables stay launchable whatever order they were made in.
+  static int cap_set = 0;
+  if (!cap_set) {
+    size_t max_smem = sizeof(float4) * ((4097 + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
+    cudaFuncSetAttribute(k_tree_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cap_set = 1;
+  }
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_walk, kWalkThreads, smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (per_sm < 1) per_sm = 1;
-  cached = per_sm * sms;
-  cached_smem = smem;
-  return cached;
+  return per_sm * sms;
 }
 
 int64_t walk_stack_words() {

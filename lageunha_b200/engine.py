@@ -44,6 +44,21 @@ class TpmParams(ctypes.Structure):
                 ("rs_split", ctypes.c_float), ("particle_mass", ctypes.c_float)]
 
 
+class TpmCosmology(ctypes.Structure):
+    _fields_ = [("omep", ctypes.c_float), ("omeplam", ctypes.c_float), ("wlam0", ctypes.c_float),
+                ("wlam1", ctypes.c_float), ("amax", ctypes.c_float)]
+
+
+class TpmEvolFact(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in ("afact", "bfact", "pfact", "fact1", "fact2", "fact1_push",
+                                              "fact2_push", "fact1_pull", "fact2_pull")]
+
+
+# WMAP5-like defaults of the reference's parameter file (Params/header.c:122-139)
+def cosmology(omep=0.26, omeplam=0.74, wlam0=-1.0, wlam1=0.0, amax=48.0) -> TpmCosmology:
+    return TpmCosmology(omep, omeplam, wlam0, wlam1, amax)
+
+
 class EngineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"tpm error {code}: {msg}")
@@ -84,6 +99,17 @@ _SIGS = {
     "tpm_read_order": (ctypes.c_int, [_P, _P, _P]),
     "tpm_read_mesh": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "tpm_morton_order_noalloc": (ctypes.c_int, [_P, _I64, ctypes.c_int32, _P, _P, _P]),
+    "tpm_graph_compute": (ctypes.c_int, [_P, ctypes.c_uint]),
+    "tpm_batch_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "tpm_batch_destroy": (ctypes.c_int, [_P]),
+    "tpm_batch_compute": (ctypes.c_int, [_P, ctypes.c_uint]),
+    "tpm_batch_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.POINTER(ctypes.c_float),
+                                      ctypes.POINTER(ctypes.c_float)]),
+    "tpm_batch_time": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float)]),
+    "tpm_evol_factors": (ctypes.c_int, [ctypes.POINTER(TpmCosmology), ctypes.c_int32, ctypes.c_float,
+                                        ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
+    "tpm_hubble_drag": (ctypes.c_int, [_P, ctypes.c_float]),
+    "tpm_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float, ctypes.c_int32]),
 }
 
 
@@ -259,6 +285,17 @@ class Engine:
         _check(self._lib.tpm_treemain(self._ctx, tdm_records.ctypes.data, tdm_records.shape[0], fact2, stepcount))
         self.np = int(tdm_records.shape[0])
 
+    def graph_compute(self, parts: int = PART_ALL):
+        """tpm_compute_forces replayed from a captured CUDA graph."""
+        _check(self._lib.tpm_graph_compute(self._ctx, parts))
+
+    def hubble_drag(self, fact1: float):
+        _check(self._lib.tpm_hubble_drag(self._ctx, fact1))
+
+    def step(self, cosmo: TpmCosmology, anow: float, astep: float, stepcount: int):
+        """One GOTPM global step in KICK status (Cosmos/globalT.c:221-305)."""
+        _check(self._lib.tpm_step(self._ctx, ctypes.byref(cosmo), anow, astep, stepcount))
+
     # ---------------------------------------------------------------- diagnostics
     def ewald(self, targets) -> np.ndarray:
         t = np.ascontiguousarray(targets, dtype=np.int64)
@@ -290,6 +327,59 @@ class Engine:
         out = np.empty(self.n_mesh ** 3, np.float32)
         _check(self._lib.tpm_read_mesh(self._ctx, which, out.ctypes.data))
         return out.reshape(self.n_mesh, self.n_mesh, self.n_mesh)
+
+
+class Batch:
+    """An ensemble of boxes (Engine objects on one device) evaluated through
+    one graph launch per call (tpm_batch_*). The engines stay usable on their
+    own; the batch must be closed before them."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        self._lib = load_library()
+        arr = (ctypes.c_void_p * len(self.engines))(*[e._ctx.value for e in self.engines])
+        b = ctypes.c_void_p()
+        _check(self._lib.tpm_batch_create(arr, len(self.engines), ctypes.byref(b)))
+        self._b = b
+
+    def close(self):
+        if self._b:
+            self._lib.tpm_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compute(self, parts: int = PART_ALL):
+        _check(self._lib.tpm_batch_compute(self._b, parts))
+
+    def step(self, cosmo: TpmCosmology, anow, astep):
+        n = len(self.engines)
+        a = (ctypes.c_float * n)(*np.broadcast_to(np.asarray(anow, np.float32), (n,)))
+        s = (ctypes.c_float * n)(*np.broadcast_to(np.asarray(astep, np.float32), (n,)))
+        _check(self._lib.tpm_batch_step(self._b, ctypes.byref(cosmo), a, s))
+
+    @property
+    def last_ms(self) -> float:
+        ms = ctypes.c_float()
+        _check(self._lib.tpm_batch_time(self._b, ctypes.byref(ms)))
+        return ms.value
+
+
+def evol_factors(cosmo: TpmCosmology, nx: int, anow: float, astep: float) -> dict:
+    """GetEvolFactor (Cosmos/CosmosEvolFactor.c:230-255); host only."""
+    out = TpmEvolFact()
+    _check(load_library().tpm_evol_factors(ctypes.byref(cosmo), nx, anow, astep, ctypes.byref(out)))
+    return {k: getattr(out, k) for k, _ in TpmEvolFact._fields_}
 
 
 def dm_records(ps) -> np.ndarray:

@@ -132,6 +132,69 @@ def plant_plummer(ps: ParticleSet, seed: int, n_spheres: int, scale_cells: float
     return ParticleSet(n, ps.box_mpc, ps.indx.copy(), offset, vel, ps.seed)
 
 
+def fft_friendly(n: int) -> int:
+    """The 2^a 3^b 5^c size nearest to n (ties to the larger)."""
+    best = None
+    for m in range(max(2, n - n // 4), n + n // 4 + 2):
+        k = m
+        for p in (2, 3, 5):
+            while k % p == 0:
+                k //= p
+        if k == 1 and (best is None or abs(m - n) < abs(best - n) or (abs(m - n) == abs(best - n) and m > best)):
+            best = m
+    return best
+
+
+@dataclasses.dataclass
+class Box:
+    """One box of an ensemble or a served request: n_lattice^3 particles on an
+    n_mesh^3 PM mesh, in the engine's uint32 fixed-point form."""
+    n_mesh: int
+    n_lattice: int
+    box_mpc: float
+    spec_index: float
+    pos: np.ndarray        # (np, 3) uint32
+    vel: np.ndarray        # (np, 3) float32, cells per unit of the drift factor
+    seed: int
+
+    @property
+    def np(self) -> int:
+        return int(self.pos.shape[0])
+
+
+def lattice_box(n_lattice: int, n_mesh: int, seed: int, spec_index: float, rms_disp: float, box_mpc: float,
+                vel_factor: float = 0.0, damp: float = 0.5) -> Box:
+    """n_lattice^3 particles displaced from their lattice by a Zel'dovich
+    field (rms displacement rms_disp lattice spacings), placed on an n_mesh^3
+    mesh: x = (q + psi) * n_mesh / n_lattice cells."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    psi = _displacement_field(n_lattice, rng, spec_index, damp, rms_disp)
+    g = np.arange(n_lattice, dtype=np.float64)
+    qz, qy, qx = np.meshgrid(g, g, g, indexing="ij")
+    scale = n_mesh / n_lattice
+    x = np.stack([(qx + psi[0]).ravel(), (qy + psi[1]).ravel(), (qz + psi[2]).ravel()], axis=1) * scale
+    vel = (vel_factor * scale * np.stack([psi[0].ravel(), psi[1].ravel(), psi[2].ravel()], axis=1)).astype(np.float32)
+    return Box(n_mesh, n_lattice, box_mpc, spec_index, to_fixed_point(np.mod(x, n_mesh), n_mesh), vel, seed)
+
+
+# The batched ensemble: 64 boxes, N_p^(1/3) log-uniform in [32, 160], mesh the
+# nearest 2^a 3^b 5^c size, L uniform in [50, 300] Mpc/h, P(k) ~ k^n with n
+# uniform in [-2.5, -1.5], rms displacement 1 spacing, v = 0.5 psi.
+ENSEMBLE_BOXES = 64
+
+
+def ensemble_box(b: int, max_lattice: int = 160, min_lattice: int = 32) -> Box:
+    rng = np.random.Generator(np.random.PCG64(4000 + b))
+    nl = int(round(np.exp(rng.uniform(np.log(min_lattice), np.log(max_lattice)))))
+    box = float(rng.uniform(50.0, 300.0))
+    ns = float(rng.uniform(-2.5, -1.5))
+    return lattice_box(nl, fft_friendly(nl), 4000 + b, ns, 1.0, box, vel_factor=0.5)
+
+
+def ensemble(nbox: int = ENSEMBLE_BOXES, max_lattice: int = 160, min_lattice: int = 32) -> list:
+    return [ensemble_box(b, max_lattice, min_lattice) for b in range(nbox)]
+
+
 def workload(name: str, scale: int | None = None) -> ParticleSet:
     """The named synthetic workloads. `scale` overrides the mesh size (for
     parity-sized cases with the same statistics).

@@ -69,6 +69,7 @@ def ref(variant: int = VARIANT_B):
         L.ref_tsc_density.argtypes = [_int, _i64, _u64p, _f32p, _f32p]
         L.ref_potential.argtypes = [_int, _i64, _u64p, _f32p, _flt, _f32p]
         L.ref_spline_table.argtypes = [_int, _flt, _f64p, _f64p]
+        L.ref_evol_factors.argtypes = [_int, _flt, _flt, _flt, _flt, _flt, _flt, _flt, _f32p]
         _ref[variant] = L
     return _ref[variant]
 
@@ -172,6 +173,15 @@ def ref_spline_table(n, eps):
     s = np.empty((4096, 3), np.float64)
     ref(VARIANT_A).ref_spline_table(n, eps, d, s)
     return d, s
+
+
+EVOL_FIELDS = ("afact", "bfact", "pfact", "fact1", "fact2", "fact1_push", "fact2_push", "fact1_pull", "fact2_pull")
+
+
+def ref_evol_factors(n, omep, omeplam, wlam0, wlam1, amax, anow, astep):
+    out = np.zeros(9, np.float32)
+    ref(VARIANT_A).ref_evol_factors(n, omep, omeplam, wlam0, wlam1, amax, anow, astep, out)
+    return dict(zip(EVOL_FIELDS, out))
 
 
 def rel_err(f, fref):

@@ -200,11 +200,6 @@ void PaddingParticles(SimParameters *simpar) {
 void CorrMeasure(SimParameters *simpar, GridInfo *g) { (void)simpar; (void)g; }
 void savexzslice(SimParameters *simpar, DenType *d) { (void)simpar; (void)d; }
 void volumeout(SimParameters *simpar, GridInfo *g, int which) { (void)simpar; (void)g; (void)which; }
-float GetFact1(SimParameters *simpar, float a, float b) {
-  (void)simpar; (void)a; (void)b;
-  fprintf(stderr, "oracle/_ref: GetFact1 (PUSH status) is not part of the oracle harness\n");
-  abort();
-}
 
 /* ------------------------------------------------------- oracle set-up */
 extern int initflag; /* Cosmos/treecorrection.c:221: spline table built once */
@@ -397,3 +392,24 @@ int ref_spline_table(int n, float eps, double *diff_out, double *slope_out) {
 }
 
 int ref_nspline(void) { return NSPLINE; }
+
+/* GetEvolFactor (Cosmos/CosmosEvolFactor.c:230-255) for one cosmology:
+ * out = {afact, bfact, pfact, fact1, fact2, fact1_push, fact2_push,
+ * fact1_pull, fact2_pull} (the EvolFact field order, CosmosEvolFactor.h:1-6). */
+int ref_evol_factors(int n, float omep, float omeplam, float wlam0, float wlam1, float amax, float anow,
+                     float astep, float *out) {
+  RefBox *b = refbox_new(n, 0.9f, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  OMEP(s) = omep;
+  OMEPLAM(s) = omeplam;
+  WLAM0(s) = wlam0;
+  WLAM1(s) = wlam1;
+  AMAX(s) = amax;
+  ANOW(s) = anow;
+  ASTEP(s) = astep;
+  EvolFact e = GetEvolFactor(s);
+  float v[9] = {e.afact, e.bfact, e.pfact, e.fact1, e.fact2, e.fact1_push, e.fact2_push, e.fact1_pull, e.fact2_pull};
+  memcpy(out, v, sizeof(v));
+  free(b);
+  return 0;
+}

@@ -17,6 +17,11 @@ Cases (all seeded, lageunha_b200.ic):
                (A and B) on a 4096-particle subsample of targets
   sparse32     300 particles at random in a 32^3 box: tree forces A and B
                (buckets with fewer than 16 sources: DirectSummation)
+  evolfact     GetEvolFactor (Cosmos/CosmosEvolFactor.c:230-255) over a grid
+               of cosmologies (LCDM, constant w, w(a) with w1 != 0), expansion
+               factors and steps
+
+    python tests/golden/make_golden.py evolfact     # one case only
 """
 import os
 import sys
@@ -32,9 +37,37 @@ from oracle import oracle as O  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
-def main():
+# (omep, omeplam, wlam0, wlam1, amax)
+EVOL_COSMOLOGIES = ((0.26, 0.74, -1.0, 0.0, 48.0), (0.26, 0.74, -0.9, 0.0, 48.0), (0.26, 0.74, -0.9, 0.2, 48.0),
+                    (0.3, 0.7, -1.1, -0.3, 31.0))
+EVOL_ANOW = (1.0, 3.0, 10.0, 24.9, 30.0, 40.0, 47.95)
+EVOL_ASTEP = (0.025, 0.1)
+EVOL_NX = 128
+
+
+def evolfact():
+    rows, facts = [], []
+    for c in EVOL_COSMOLOGIES:
+        for anow in EVOL_ANOW:
+            if anow >= c[4]:
+                continue
+            for astep in EVOL_ASTEP:
+                r = O.ref_evol_factors(EVOL_NX, *c, anow, astep)
+                rows.append((*c, anow, astep))
+                facts.append([r[k] for k in O.EVOL_FIELDS])
+    np.savez_compressed(os.path.join(OUT, "evolfact.npz"), nx=EVOL_NX, fields=np.array(O.EVOL_FIELDS),
+                        cases=np.array(rows, np.float32), factors=np.array(facts, np.float32))
+
+
+def main(which=None):
     if not (O.ref_available(O.VARIANT_A) and O.ref_available(O.VARIANT_B)):
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` where the reference tree exists")
+    if which == "evolfact":
+        evolfact()
+        return
+    if which is not None:
+        raise SystemExit(f"unknown case {which}")
+    evolfact()
 
     # ---- plain16
     n = 16
@@ -72,9 +105,9 @@ def main():
     fb = O.ref_tree_force(n, indx, off, variant=O.VARIANT_B, eps=0.05)
     np.savez_compressed(os.path.join(OUT, "sparse32.npz"), n=n, indx=indx, offset=off, tree_force_A=fa,
                         tree_force_B=fb)
-    for f in ("plain16.npz", "clustered32.npz", "sparse32.npz"):
+    for f in ("plain16.npz", "clustered32.npz", "sparse32.npz", "evolfact.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)
