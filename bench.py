@@ -12,9 +12,11 @@ theta 0.3.
 The metric is quoted at rms force error <= 1e-3 against the FP64 Ewald sum.
 The reference's own split law (PMFITPARA residual, efold 0.9, rsphere 4)
 stays near 3.5e-3 on this workload, so the headline uses the engine's
-Gaussian split (rs = 1.2 cells, short-range cut at 6 cells, 8-point
-gradient), which measures rms ~6e-4; the same line also carries the
-reference law's throughput and error ("reference_law").
+Gaussian split (rs = 0.9 cells, short-range cut at 4.5 cells, interlaced
+TSC grids, 8-point gradient, theta 0.4); the same line also carries the
+reference law's throughput and error ("reference_law"), one KDK global step
+("kdk_step_ms"), the 64-box uneven ensemble evaluated box by box and batched
+("ensemble"), and the served request loop ("served").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -43,7 +45,10 @@ sys.path.insert(0, ROOT)
 METRIC = "Mparticles/s per TreePM force eval (plain vs batched) at rms err≤1e-3; p50/p99 latency"
 UNIT = "Mparticles/s"
 EPS = 0.05
-HEADLINE_LAW = {"law": "gaussian", "rs_split": 1.2, "rsphere": 6.0, "theta": 0.3, "efold": 0.9}
+HEADLINE_LAW = {"law": "gaussian", "rs_split": 0.9, "rsphere": 4.5, "theta": 0.4, "efold": 0.9}
+# weakly clustered boxes carry small net forces: the ensemble and the served
+# requests open nodes more often to stay under the same error bar
+BOX_LAW = {"law": "gaussian", "rs_split": 0.9, "rsphere": 4.5, "theta": 0.3, "efold": 0.9}
 REFERENCE_LAW = {"law": "reference", "rs_split": 1.25, "rsphere": 4.0, "theta": 0.3, "efold": 0.9}
 FP32_LANES_PER_SM = 128
 # FLOPs charged per evaluated interaction of the walk (DESIGN.md derives them):
@@ -198,6 +203,138 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- engine arm
+def run_batched(args, E, ic, law, local):
+    """The 64-box uneven ensemble: every box through the plain engine one
+    after another (each call synchronises, as a caller of the plain engine
+    does), then the same boxes as one ensemble (one graph launch per
+    evaluation). Both evaluate the same forces with the same law."""
+    import torch
+    t0 = time.time()
+    boxes = ic.ensemble(args.ensemble_boxes)
+    t_ic = time.time() - t0
+    engines = [E.Engine(b.n_mesh, epsilon=EPS, device=local, **law) for b in boxes]
+    for e, b in zip(engines, boxes):
+        e.load_fixed(b.pos, b.vel)
+    for e in engines:
+        e.sync()
+    total = sum(b.np for b in boxes)
+
+    def plain():
+        for e in engines:
+            e.compute(E.PART_ALL)
+
+    batch = E.Batch(engines)
+    plain()
+    batch.compute(E.PART_ALL)
+    reps = 3
+    tp = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        s = time.perf_counter()
+        plain()
+        tp.append(time.perf_counter() - s)
+    tb, tbd = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        s = time.perf_counter()
+        batch.compute(E.PART_ALL)
+        tb.append(time.perf_counter() - s)
+        tbd.append(batch.last_ms * 1e-3)
+    ms_step = None
+    cosmo = E.cosmology()
+    batch.step(cosmo, 5.0, 0.02)
+    ms_step = batch.last_ms
+    # accuracy: FP64 Ewald on 1024 targets of a small, a middle and the largest box
+    order = sorted(range(len(boxes)), key=lambda i: boxes[i].np)
+    errs = []
+    batch.compute(E.PART_ALL)
+    for i in (order[0], order[len(order) // 2], order[-1]):
+        b, e = boxes[i], engines[i]
+        f = e.forces()
+        rng = np.random.Generator(np.random.PCG64(1024 + i))
+        tg = np.sort(rng.choice(b.np, min(1024, b.np), replace=False)).astype(np.int64)
+        few = e.ewald(tg)
+        er = np.linalg.norm(f[tg].astype(np.float64) - few, axis=1) / np.linalg.norm(few, axis=1)
+        errs.append({"n_lattice": b.n_lattice, "n_mesh": b.n_mesh, "rms": float(np.sqrt(np.mean(er * er))),
+                     "p99": float(np.percentile(er, 99))})
+    batch.close()
+    for e in engines:
+        e.close()
+    plain_s, batch_s = min(tp), min(tb)
+    return {
+        "boxes": len(boxes), "particles": total,
+        "lattice_range": [min(b.n_lattice for b in boxes), max(b.n_lattice for b in boxes)],
+        "meshes": sorted({b.n_mesh for b in boxes}),
+        "plain_box_by_box": {"value": total / plain_s / 1e6, "ms": plain_s * 1e3},
+        "batched": {"value": total / batch_s / 1e6, "ms": batch_s * 1e3, "device_ms": min(tbd) * 1e3},
+        "speedup": plain_s / batch_s,
+        "kdk_step_ms": ms_step,
+        "err_vs_ewald": errs,
+        "ic_seconds": t_ic,
+        "unit": UNIT,
+        "timing": "wall clock around each whole-ensemble evaluation after a device synchronize (best of 3); "
+                  "device_ms from CUDA events around the ensemble graph launch",
+    }
+
+
+def run_served(args, E, ic, law, local):
+    """Served solves: seeded Poisson arrivals (mean 200 requests/s) of boxes
+    drawn log-uniform in 32^3..256^3 particles with 1-20 global steps each,
+    submitted to the request loop at their arrival times; latency = done -
+    arrival per request; throughput = particle-steps / (last done - first
+    arrival)."""
+    rng = np.random.Generator(np.random.PCG64(5))
+    nreq = args.served_requests
+    gaps = rng.exponential(1.0 / 200.0, nreq)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    reqs = []
+    t0 = time.time()
+    for r in range(nreq):
+        rr = np.random.Generator(np.random.PCG64(5000 + r))
+        nl = int(round(np.exp(rr.uniform(np.log(32), np.log(256)))))
+        nsteps = int(rr.integers(1, 21))
+        ns = float(rr.uniform(-2.5, -1.5))
+        box = ic.lattice_box(nl, ic.fft_friendly(nl), 5000 + r, ns, 1.0, float(rr.uniform(50, 300)), vel_factor=0.5)
+        reqs.append((box, nsteps))
+    t_ic = time.time() - t0
+    import torch
+    pinned = []
+    for box, _ in reqs:
+        pos = torch.from_numpy(box.pos.view(np.int32)).pin_memory()
+        vel = torch.from_numpy(box.vel).pin_memory()
+        po = torch.empty((box.np, 3), dtype=torch.int32).pin_memory()
+        vo = torch.empty((box.np, 3), dtype=torch.float32).pin_memory()
+        pinned.append((pos, vel, po, vo))
+    cosmo = E.cosmology()
+    srv = E.Server(hbm_cap_bytes=150 * 10 ** 9, max_active=64, device=local)
+    ids = []
+    start = time.perf_counter()
+    for r, ((box, nsteps), (pos, vel, po, vo)) in enumerate(zip(reqs, pinned)):
+        delay = arrivals[r] - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(pos.numpy().view(np.uint32), vel.numpy(), n_mesh=box.n_mesh, nsteps=nsteps, anow=4.0,
+                              astep=0.02, cosmo=cosmo, pos_out=po.numpy().view(np.uint32), vel_out=vo.numpy(),
+                              epsilon=EPS, **law))
+    srv.wait(-1, 3600.0)
+    infos = [srv.info(i) for i in ids]
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([i.t_done - i.t_submit for i in infos])
+    wait = np.array([i.t_admit - i.t_submit for i in infos])
+    span = max(i.t_done for i in infos) - min(i.t_submit for i in infos)
+    work = sum(box.np * ns for box, ns in reqs)
+    failed = sum(1 for i in infos if i.state != E.REQ_DONE)
+    return {
+        "requests": nreq, "failed": failed, "arrival_rate_per_s": 200,
+        "particle_steps": int(work), "value": work / span / 1e6, "unit": "Mparticle-steps/s",
+        "span_s": span,
+        "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3)},
+        "admission_wait_ms": {"p50": float(np.percentile(wait, 50) * 1e3), "p99": float(np.percentile(wait, 99) * 1e3)},
+        "server": stats, "hbm_cap_bytes": 150 * 10 ** 9, "ic_seconds": t_ic,
+    }
+
+
 def run_engine_arm(args):
     import torch
     from lageunha_b200 import engine as E
@@ -383,9 +520,26 @@ def run_engine_arm(args):
         "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
                    "reasons": clocks.get("reasons", [])},
     }
+    # ---- one KDK global step of the same box (drag, forces, kicks, drift)
+    cosmo = E.cosmology()
+    eng.load_fixed(pos_dev)
+    eng.step(cosmo, 5.0, 0.02, 0)
+    barrier()
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    eng.step(cosmo, 5.02, 0.02, 1)
+    k1.record(stream)
+    barrier()
+    line["kdk_step_ms"] = k0.elapsed_time(k1)
+    eng.close()
+    box_law = REFERENCE_LAW if args.law == "reference" else BOX_LAW
+    if not args.no_batched:
+        line["ensemble"] = {"law": box_law, **run_batched(args, E, ic, box_law, local)}
+    if not args.no_served:
+        line["served"] = {"law": box_law, **run_served(args, E, ic, box_law, local)}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
-    eng.close()
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
@@ -408,6 +562,10 @@ def main():
     ap.add_argument("--no-reference-law", action="store_true")
     ap.add_argument("--no-ewald", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-box ensemble block")
+    ap.add_argument("--no-served", action="store_true", help="skip the served request-loop block")
+    ap.add_argument("--ensemble-boxes", type=int, default=64)
+    ap.add_argument("--served-requests", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -208,6 +208,56 @@ int tpm_batch_step(tpm_batch *batch, const tpm_cosmology *cosmo, const float *an
 /* Device time of the last tpm_batch_compute / tpm_batch_step launch, ms. */
 int tpm_batch_time(tpm_batch *batch, float *ms);
 
+/* ---- the request loop (served solves) ---- */
+
+/* A worker thread on one device admits requests in arrival order while
+ * their device footprint fits under hbm_cap_bytes and in the free HBM, keeps
+ * each request's particles, mesh and tree on the device between its steps,
+ * and runs the active requests' steps as they become ready, so requests that
+ * arrive while others run overlap with them on the device. No counterpart in
+ * the reference (a batch MPI job). */
+typedef struct tpm_server tpm_server;
+
+typedef struct tpm_request {
+  tpm_params params;       /* the box's parameters (n_mesh, law, ...) */
+  int64_t np;
+  const uint32_t *pos;     /* host [np][3] fixed point, valid until done */
+  const float *vel;        /* host [np][3] or NULL (zeros) */
+  tpm_cosmology cosmo;
+  float anow, astep;       /* step k runs at anow + k*astep */
+  int32_t nsteps;          /* 0: one force evaluation; n >= 1: n global steps */
+  uint32_t *pos_out;       /* host [np][3] or NULL: positions after the steps */
+  float *vel_out;          /* host [np][3] or NULL: velocities after the steps */
+  float *force_out;        /* host [np][3] or NULL: forces of the last evaluation */
+} tpm_request;
+
+#define TPM_REQ_QUEUED 0
+#define TPM_REQ_ACTIVE 1
+#define TPM_REQ_DONE 2
+#define TPM_REQ_FAILED 3
+
+typedef struct tpm_request_info {
+  int32_t state;           /* TPM_REQ_* */
+  int32_t status;          /* TPM_OK, or the error of a failed request */
+  double t_submit, t_admit, t_done;  /* seconds since the server was created */
+  int64_t device_bytes;    /* device memory held while active */
+} tpm_request_info;
+
+/* Device bytes a context for this mesh and particle count holds. */
+int64_t tpm_estimate_bytes(int32_t n_mesh, int64_t np);
+int tpm_server_create(int device, int64_t hbm_cap_bytes, int32_t max_active, tpm_server **out);
+/* Non-blocking; the request's host buffers must stay valid until it is done. */
+int tpm_server_submit(tpm_server *server, const tpm_request *req, int64_t *id);
+int tpm_server_info(tpm_server *server, int64_t id, tpm_request_info *out);
+/* Waits for request id (id < 0: every request submitted so far). */
+int tpm_server_wait(tpm_server *server, int64_t id, double timeout_s);
+/* [0] done [1] failed [2] peak active [3] peak device bytes [4] contexts
+ * created [5] contexts reused [6] contexts evicted [7] deferred admissions;
+ * returns the number of words written. */
+int tpm_server_stats(tpm_server *server, int64_t *out, int n);
+/* Finishes every submitted request, then stops the worker. */
+int tpm_server_destroy(tpm_server *server);
+
 /* ---- diagnostics ---- */
 
 /* FP64 periodic Ewald force (reference units, Plummer softening epsilon on

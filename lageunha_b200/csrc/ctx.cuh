@@ -59,6 +59,11 @@ struct tpm_ctx {
   float2 *spec = nullptr;
   float *phi = nullptr;
   CUtensorMap tmap2, tmap4;  // potential boxes for the 4- and 8-point gradients
+  // the half-cell-shifted grid of the interlaced deposit (Gaussian law)
+  float *rho2 = nullptr;
+  float2 *spec2 = nullptr;
+  float *phi2 = nullptr;
+  CUtensorMap tmap4b;
   uint32_t *tile_start = nullptr;
   // tree
   tpm::TreeBuffers tb;
@@ -109,6 +114,12 @@ int finish_forces(tpm_ctx *c, unsigned parts, bool from_host, bool timing);
 int launch_drag(tpm_ctx *c, cudaStream_t st, float fact1, const double *fac);
 int launch_kick(tpm_ctx *c, cudaStream_t st, float f2pm, float f2tree, const double *fac);
 int launch_drift(tpm_ctx *c, cudaStream_t st, double pfact, const double *fac);
+// k_finish into c->fout: the summed forces in the caller's particle order.
+int launch_finish(tpm_ctx *c, cudaStream_t st);
+// Device bytes a context of this mesh and particle capacity allocates.
+int64_t ctx_bytes(int n_mesh, int64_t np);
+// Parameter validation of tpm_create / tpm_set_params (sets the error).
+int check_params(const tpm_params *p);
 // The reference's opening-angle schedule (Cosmos/globalT.c:41-44).
 float theta_schedule(int stepcount);
 // Makes c->graphs[kind] current (captures it again after a change).

@@ -76,7 +76,7 @@ const char *tpm_version(void) { return "lageunha_b200 tpm_engine 0.1 (sm_100a)";
 
 }  // extern "C"
 
-static int check_params(const tpm_params *p) {
+int tpm::check_params(const tpm_params *p) {
   if (!p) return fail(TPM_E_ARG, "params is NULL");
   if (p->n_mesh < 16 || p->n_mesh > 4096) return fail(TPM_E_ARG, "n_mesh %d outside [16, 4096]", p->n_mesh);
   if (p->law != TPM_LAW_REFERENCE && p->law != TPM_LAW_GAUSSIAN) return fail(TPM_E_ARG, "unknown law %d", p->law);
@@ -181,7 +181,31 @@ static int build_law(tpm_ctx *c) {
 }
 
 // ------------------------------------------------------------------ buffers
+static void free_mesh2(tpm_ctx *c) {
+  if (c->rho2) cudaFree(c->rho2);
+  if (c->spec2) cudaFree(c->spec2);
+  if (c->phi2) cudaFree(c->phi2);
+  c->rho2 = nullptr;
+  c->spec2 = nullptr;
+  c->phi2 = nullptr;
+}
+
+// The second (half-cell-shifted) grid of the Gaussian law's interlaced PM.
+static int ensure_mesh2(tpm_ctx *c) {
+  if (c->prm.law != TPM_LAW_GAUSSIAN || c->rho2) return 0;
+  const MeshGeom &g = c->g;
+  int64_t n3 = (int64_t)g.n * g.n * g.n;
+  CK(cudaMalloc(&c->rho2, sizeof(float) * n3));
+  CK(cudaMalloc(&c->spec2, sizeof(float2) * g.spec_elems));
+  CK(cudaMalloc(&c->phi2, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  CK(cudaMemsetAsync(c->phi2, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz, c->st));
+  if (make_phi_tensor_map(g, c->phi2, 4, &c->tmap4b) != 0) return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
+  c->gen++;
+  return 0;
+}
+
 static void free_mesh(tpm_ctx *c) {
+  free_mesh2(c);
   if (c->rho) cudaFree(c->rho);
   if (c->spec) cudaFree(c->spec);
   if (c->phi) cudaFree(c->phi);
@@ -398,6 +422,29 @@ int grid_for(int64_t n, int threads = 256) {
 
 }  // namespace
 
+int tpm::launch_finish(tpm_ctx *c, cudaStream_t st) {
+  k_finish<<<grid_for(c->np), 256, 0, st>>>(c->perm, c->np, c->fpm, c->ftree, TPM_PART_ALL, c->fout);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int64_t tpm::ctx_bytes(int n_mesh, int64_t np) {
+  // the allocations of tpm_create, alloc_mesh and ensure_particles
+  MeshGeom g = make_geom(n_mesh);
+  int64_t n3 = (int64_t)g.n * g.n * g.n;
+  // both grids of the interlaced pair (the Gaussian law's second grid)
+  int64_t mesh = 2 * (4 * n3 + 8 * g.spec_elems + 4 * (int64_t)g.px * g.py * g.pz);
+  int64_t ntiles = 1ll << (3 * (g.cbits - 3)), ncubes = 1ll << (3 * (g.cbits - 2));
+  mesh += 4 * (ntiles + 1) + 4 * (ncubes + 1) + 8 * (int64_t)(n_mesh + n_mesh / 2 + 1);
+  int64_t parts = np * (12 + 12 + 8 + 8 + 4 + 4 + 12 + 12 + 12 + 12) + 4 * 256 * (sort_tiles(np) + 1) + 1024;
+  int64_t cap_nodes = np + np / 4 + 64;
+  int64_t tree = cap_nodes * (4 + 4 + 4 + 4 + 1 + 16 + 3 * 16 + 32 + 16);
+  int64_t ts = (cap_nodes + 1023) / 1024 + 16, need = 2 * ncubes + (ncubes + 4095) / 4096 + 16;
+  tree += 4 * (ts > need ? ts : need) + 8 * (np + ncubes + 16);
+  int64_t fixed = 4 * walk_stack_words() + 8 * 4097 + 16 * 4096 + 4096;
+  return mesh + parts + tree + fixed;
+}
+
 int tpm::launch_drag(tpm_ctx *c, cudaStream_t st, float fact1, const double *fac) {
   k_drag<<<grid_for(3 * c->np), 256, 0, st>>>(c->vel, 3 * c->np, fact1, fac);
   CK(cudaGetLastError());
@@ -441,6 +488,7 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
     return fail(TPM_E_CUDA, "cudaStreamCreate failed");
   }
   for (int i = 0; i <= kNStages; i++) cudaEventCreate(&c->ev[i]);
+  // the allocations below are mirrored by ctx_bytes()
   if (cudaMalloc(&c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
       cudaMalloc(&c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
       cudaMalloc(&c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess) {
@@ -462,6 +510,7 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
   memset(c->hfac, 0, sizeof(double) * kFacWords);
   cudaMemsetAsync(c->err, 0, sizeof(uint32_t) * 8, c->st);
   rc = alloc_mesh(c);
+  if (!rc) rc = ensure_mesh2(c);
   if (!rc) rc = build_law(c);
   if (rc) {
     std::string m = g_err;
@@ -514,6 +563,8 @@ int tpm_set_params(tpm_ctx *c, const tpm_params *p) {
     rc = alloc_mesh(c);
     if (rc) return rc;
   }
+  rc = ensure_mesh2(c);
+  if (rc) return rc;
   c->parts_valid = 0;
   return build_law(c);
 }
@@ -604,20 +655,34 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     uint32_t ntiles = 1u << (3 * (g.cbits - 3));
     launch_range_table(c->skey, np, 3 * (g.sub_bits + 3), ntiles, c->tile_start, st);
     CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
-    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st);
+    const bool il = c->prm.law == TPM_LAW_GAUSSIAN;  // interlaced pair of grids
+    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st, 0);
     c->launches += 2;
+    if (il) {
+      CK(cudaMemsetAsync(c->rho2, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
+      launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho2, st, 1);
+      c->launches += 1;
+    }
     CK(stage_check(st, "deposit"));
     if (timing) CK(cudaEventRecord(c->ev[2], st));
-    launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st, &c->launches);
+    if (il)
+      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
+                     &c->launches, c->rho2, c->spec2, c->phi2);
+    else
+      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
+                     &c->launches);
     CK(stage_check(st, "fft"));
     if (timing) CK(cudaEventRecord(c->ev[3], st));
     // the reference law keeps the reference's 4-point gradient; the Gaussian
-    // law uses the 8-point one
-    if (c->prm.law == TPM_LAW_REFERENCE)
+    // law uses the 8-point one on both interlaced grids and averages
+    if (c->prm.law == TPM_LAW_REFERENCE) {
       launch_fda4(g, &c->tmap2, 2, c->spos, c->tile_start, c->fpm, c->err, st);
-    else
-      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, st);
-    c->launches += 1;
+      c->launches += 1;
+    } else {
+      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, st, 0, 0);
+      launch_fda4(g, &c->tmap4b, 4, c->spos, c->tile_start, c->fpm, c->err, st, 1, 1);
+      c->launches += 2;
+    }
     CK(stage_check(st, "fda4"));
     if (timing) CK(cudaEventRecord(c->ev[4], st));
   } else if (timing) {
@@ -838,6 +903,11 @@ int tpm_counters(tpm_ctx *c, int64_t *out, int n) {
 }
 
 int64_t tpm_launch_count(tpm_ctx *c) { return c ? c->launches : 0; }
+
+int64_t tpm_estimate_bytes(int32_t n_mesh, int64_t np) {
+  if (n_mesh < 16 || n_mesh > 4096 || np <= 0) return -1;
+  return ctx_bytes(n_mesh, np);
+}
 
 int tpm_read_order(tpm_ctx *c, uint64_t *keys, uint32_t *perm) {
   if (!c) return fail(TPM_E_ARG, "ctx is NULL");

@@ -56,8 +56,10 @@ constexpr int kGhost = 8;    // ghost layers of the padded potential (8-point st
 
 MeshGeom make_geom(int n);
 
+// half != 0 deposits the particles moved by half a cell along every axis (the
+// second grid of the interlaced pair).
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
-                        float mass, float *rho, cudaStream_t st);
+                        float mass, float *rho, cudaStream_t st, int half);
 // FFT pipeline: rho (n^3 real) -> phi_pad (ghosted potential).
 struct FftPlan {
   float2 *tw = nullptr;   // twiddles exp(-2 pi i k / L) for L = n and L = n/2
@@ -67,12 +69,19 @@ struct FftPlan {
 // twiddle tables are written on st
 void fft_plan_init(FftPlan &p, int n, cudaStream_t st);
 void fft_plan_free(FftPlan &p);
+// With rho2 (the half-cell-shifted deposit) the two grids are interlaced:
+// their spectra are combined before the Green's function and phi2_pad gets
+// the potential on the shifted grid.
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
-                    int64_t *launches);
+                    int64_t *launches, const float *rho2 = nullptr, float2 *spec2 = nullptr,
+                    float *phi2_pad = nullptr);
 // fda4: gradient and TSC interpolation per tile through TMA.
+// half: positions moved by half a cell (the shifted grid); average: write the
+// mean of the new force and the one already in fpm.
 void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
-                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st);
+                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st, int half = 0,
+                 int average = 0);
 // Tensor maps of the potential for the 4-point (radius 2) and the 8-point
 // (radius 4) gradient: their boxes differ.
 int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorMap *out);

@@ -46,8 +46,11 @@ struct Axis {
   float xmin;   // x - near in [-0.5, 0.5]
 };
 
-TPM_D Axis axis_of(uint32_t u, uint32_t n) {
-  uint64_t p = (uint64_t)u * (uint64_t)n;
+// half != 0: the position moved by exactly half a cell along the axis (the
+// second grid of the interlaced deposit), without the periodic wrap, so a
+// particle keeps the home-node range [8t, 8t+8] of its Morton tile t.
+TPM_D Axis axis_of(uint32_t u, uint32_t n, uint32_t half = 0) {
+  uint64_t p = (uint64_t)u * (uint64_t)n + (half ? 0x80000000ull : 0ull);
   int c = (int)(p >> 32);
   uint32_t fr = (uint32_t)p;
   Axis a;
@@ -76,7 +79,7 @@ constexpr int kDepThreads = 256;
 
 __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
     const uint32_t *__restrict__ spos, const uint32_t *__restrict__ tile_start, int n, int cbits,
-    float mass, float *__restrict__ rho, int vec4) {
+    float mass, float *__restrict__ rho, int vec4, uint32_t half) {
   __shared__ float acc[kDepCells];
   int tid = threadIdx.x, lane = tid & 31;
   // Morton tile index -> tile coordinates
@@ -102,8 +105,8 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
     int hx = 0, hy = 0, hz = 0;
     if (valid) {
       int64_t i = (int64_t)p0 + k;
-      Axis ax = axis_of(spos[3 * i + 0], nu), ay = axis_of(spos[3 * i + 1], nu),
-           az = axis_of(spos[3 * i + 2], nu);
+      Axis ax = axis_of(spos[3 * i + 0], nu, half), ay = axis_of(spos[3 * i + 1], nu, half),
+           az = axis_of(spos[3 * i + 2], nu, half);
       float w1, w2, w3;
       int s;
       tsc_w(ax.xmin, w1, w2, w3, s);
@@ -199,10 +202,11 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
 }
 
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
-                        float mass, float *rho, cudaStream_t st) {
+                        float mass, float *rho, cudaStream_t st, int half) {
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
   int vec4 = (g.n % 4) == 0;
-  k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho, vec4);
+  k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho, vec4,
+                                                (uint32_t)half);
 }
 
 // ------------------------------------------------------------------ FFT
@@ -383,8 +387,9 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
 __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__ phi, struct FftArgs a,
                             const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n, int64_t nrows,
                             int px, int py);
-__global__ void k_fft_cols(float2 *__restrict__ spec, struct FftArgs a, const float2 *__restrict__ tw_n, int axis,
-                           float dir, int with_green, struct GreenArgs ga, int TX);
+__global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2, struct FftArgs a,
+                           const float2 *__restrict__ tw_n, int axis, float dir, int with_green, struct GreenArgs ga,
+                           int TX, int nspec);
 
 void fft_plan_init(FftPlan &p, int n, cudaStream_t st) {
   p.n = n;
@@ -490,10 +495,18 @@ TPM_D float green(const GreenArgs &g, int kx, int ky, int kz) {
   return fact / wave * expf(-wave * g.rs2k) * g.irngc / s;
 }
 
-__global__ void k_fft_cols(float2 *__restrict__ spec, FftArgs a, const float2 *__restrict__ tw_n,
-                           int axis, float dir, int with_green, GreenArgs ga, int TX) {
+// nspec == 2: the same columns of a second spectrum (the interlaced grid) go
+// through the transform as TX more pencils; with the Green's function the two
+// are combined, rho = (rho1 + e^{i k.s} rho2) / 2 with s = (1/2, 1/2, 1/2)
+// cells, which cancels the odd alias images of the TSC assignment, and the
+// potential goes back to both grids, phi1 = G rho and phi2 = e^{-i k.s} G rho.
+// Nyquist planes of an even mesh, where the shift phase is ambiguous, are
+// zeroed.
+__global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2, FftArgs a,
+                           const float2 *__restrict__ tw_n, int axis, float dir, int with_green, GreenArgs ga,
+                           int TX, int nspec) {
   extern __shared__ float2 sm[];
-  int n = a.n, hx = a.hx, L = n, P = TX;
+  int n = a.n, hx = a.hx, L = n, P = TX * nspec;
   float2 *twl = sm;
   float2 *A = sm + L;
   float2 *B = A + P * L;
@@ -506,27 +519,49 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, FftArgs a, const float2 *_
   int64_t base = axis == 1 ? (int64_t)outer * n * hx : (int64_t)outer * hx;
   int tw_ = min(TX, hx - kx0);
   for (int e = tid; e < P * L; e += nth) {
-    int q = e % TX, m = e / TX;  // consecutive threads -> consecutive kx
+    int q = e % P, m = e / P;  // consecutive threads -> consecutive kx
+    int qs = q % TX;
+    const float2 *src = q < TX ? spec : spec2;
     float2 v = make_float2(0.f, 0.f);
-    if (q < tw_) v = spec[base + m * stride + kx0 + q];
+    if (qs < tw_) v = src[base + m * stride + kx0 + qs];
     A[q * L + m] = v;
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, P, dir, a.radix, a.nf);
   if (with_green) {
-    for (int e = tid; e < P * L; e += nth) {
-      int q = e / L, m = e - q * L;
-      float gk = green(ga, kx0 + q, outer, m);
-      float2 v = res[e];
-      res[e] = make_float2(v.x * gk, v.y * gk);
+    if (nspec == 1) {
+      for (int e = tid; e < P * L; e += nth) {
+        int q = e / L, m = e - q * L;
+        float gk = green(ga, kx0 + q, outer, m);
+        float2 v = res[e];
+        res[e] = make_float2(v.x * gk, v.y * gk);
+      }
+    } else {
+      int wy = outer > n / 2 ? outer - n : outer;
+      for (int e = tid; e < TX * L; e += nth) {
+        int q = e / L, m = e - q * L;
+        int kx = kx0 + q, wz = m > n / 2 ? m - n : m;
+        float gk = green(ga, kx, outer, m);
+        if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
+        float s, c;
+        sincospif((float)(kx + wy + wz) / (float)n, &s, &c);
+        float2 r1 = res[e], r2 = res[e + TX * L];
+        // (rho1 + e^{i theta} rho2) / 2, then times G
+        float2 rho = make_float2(0.5f * (r1.x + c * r2.x - s * r2.y), 0.5f * (r1.y + c * r2.y + s * r2.x));
+        float2 ph = make_float2(rho.x * gk, rho.y * gk);
+        res[e] = ph;
+        res[e + TX * L] = make_float2(c * ph.x + s * ph.y, c * ph.y - s * ph.x);  // e^{-i theta} phi
+      }
     }
     __syncthreads();
     float2 *other = res == A ? B : A;
     res = fft_pencils(res, other, twl, L, P, 1.f, a.radix, a.nf);
   }
   for (int e = tid; e < P * L; e += nth) {
-    int q = e % TX, m = e / TX;
-    if (q < tw_) spec[base + m * stride + kx0 + q] = res[q * L + m];
+    int q = e % P, m = e / P;
+    int qs = q % TX;
+    float2 *dst = q < TX ? spec : spec2;
+    if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * L + m];
   }
 }
 
@@ -608,9 +643,21 @@ static int pencils_for(int L) {
   return P;
 }
 
+// Columns per block of the y and z passes: 8 (16 below n = 256) consecutive
+// kx, fewer where the block's shared memory (twiddles + two buffers of
+// nspec * TX pencils) would exceed 160 KB.
+static int cols_per_block(int n, int hx, int nspec) {
+  int TX = n >= 256 ? 8 : 16;
+  int tmax = (int)(((160 * 1024) / (int)sizeof(float2) / n - 1) / (2 * nspec));
+  if (TX > tmax) TX = tmax;
+  if (TX > hx) TX = hx;
+  if (TX < 1) TX = 1;
+  return TX;
+}
+
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
-                    int64_t *launches) {
+                    int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad) {
   int n = g.n;
   int64_t nrows = (int64_t)n * n;
   bool packed = (n % 2) == 0;
@@ -620,12 +667,13 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   const float2 *twL = packed ? p.tw_half : p.tw;
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
   int thx = 256;
+  int nspec = rho2 ? 2 : 1;
   k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho, spec, ax, twL, p.tw, nrows);
+  if (rho2) k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho2, spec2, ax, twL, p.tw, nrows);
   // columns
-  int TX = n >= 256 ? 8 : 16;
-  if (TX > g.hx) TX = g.hx;
-  FftArgs ac = fft_args(n, n, TX);
-  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  int TX = cols_per_block(n, g.hx, nspec);
+  FftArgs ac = fft_args(n, n, TX * nspec);
+  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * n);
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   ga.law = law;
@@ -633,12 +681,15 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   ga.sfact = (float)(-pow(M_PI * (double)efold / (double)n, 2));
   ga.irngc = (float)(1.0 / ((double)n * n * n));
   ga.rs2k = (float)pow(2.0 * M_PI * (double)rs_split / (double)n, 2);
-  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 1, -1.f, 0, ga, TX);
-  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 2, -1.f, 1, ga, TX);
-  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, ac, p.tw, 1, 1.f, 0, ga, TX);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, -1.f, 0, ga, TX, nspec);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 2, -1.f, 1, ga, TX, nspec);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, 1.f, 0, ga, TX, nspec);
   k_fft_x_c2r<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(spec, phi_pad, ax, twL, p.tw, nrows,
                                                                      g.px, g.py);
-  if (launches) *launches += 5;
+  if (rho2)
+    k_fft_x_c2r<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(spec2, phi2_pad, ax, twL, p.tw, nrows,
+                                                                       g.px, g.py);
+  if (launches) *launches += rho2 ? 7 : 5;
 }
 
 // ------------------------------------------------------------------ fda4
@@ -681,7 +732,7 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
                                                       const uint32_t *__restrict__ spos,
                                                       const uint32_t *__restrict__ tile_start, int n,
                                                       int cbits, float *__restrict__ fpm,
-                                                      uint32_t *__restrict__ err) {
+                                                      uint32_t *__restrict__ err, uint32_t half, int average) {
   using B = FdaBox<R>;
   // dynamic shared memory: the potential box (128-byte aligned for TMA), then
   // the three gradient components
@@ -753,8 +804,8 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
   __syncthreads();
   uint32_t nu = (uint32_t)n;
   for (uint32_t k = p0 + tid; k < p1; k += kFdaThreads) {
-    Axis ax = axis_of(spos[3 * (int64_t)k + 0], nu), ay = axis_of(spos[3 * (int64_t)k + 1], nu),
-         az = axis_of(spos[3 * (int64_t)k + 2], nu);
+    Axis ax = axis_of(spos[3 * (int64_t)k + 0], nu, half), ay = axis_of(spos[3 * (int64_t)k + 1], nu, half),
+         az = axis_of(spos[3 * (int64_t)k + 2], nu, half);
     float wx1, wx2, wx3, wy1, wy2, wy3, wz1, wz2, wz3;
     int sx, sy, sz;
     tsc_w(ax.xmin, wx1, wx2, wx3, sx);
@@ -780,6 +831,12 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
           fz += wt * gz[node];
         }
       }
+    if (average) {
+      // the second grid of the interlaced pair: mean of the two grids' forces
+      fx = 0.5f * (fpm[3 * (int64_t)k + 0] + fx);
+      fy = 0.5f * (fpm[3 * (int64_t)k + 1] + fy);
+      fz = 0.5f * (fpm[3 * (int64_t)k + 2] + fz);
+    }
     fpm[3 * (int64_t)k + 0] = fx;
     fpm[3 * (int64_t)k + 1] = fy;
     fpm[3 * (int64_t)k + 2] = fz;
@@ -819,17 +876,19 @@ int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorM
 }
 
 void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
-                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st) {
+                 const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st, int half, int average) {
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
   const size_t nodes = sizeof(float) * 3 * kNodes * kNodes * kNodes;
   if (radius == 2) {
     size_t smem = sizeof(float) * FdaBox<2>::BY * FdaBox<2>::BY * FdaBox<2>::BX + nodes;
     cudaFuncSetAttribute(k_fda4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fda4<2><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+    k_fda4<2><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err,
+                                                 (uint32_t)half, average);
   } else {
     size_t smem = sizeof(float) * FdaBox<4>::BY * FdaBox<4>::BY * FdaBox<4>::BX + nodes;
     cudaFuncSetAttribute(k_fda4<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fda4<4><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err);
+    k_fda4<4><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err,
+                                                 (uint32_t)half, average);
   }
 }
 

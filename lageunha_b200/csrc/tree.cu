@@ -513,9 +513,23 @@ TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, cons
   az = fmaf(dz, f, az);
 }
 
-TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpi,
-                   float rs2, const float2 *__restrict__ t0, float wmax, unsigned long long &npp) {
+// The group's bounding box (cells, relative to u_ref) and the squared reach
+// beyond it: a source farther than that from the box is outside rsphere of
+// every target of the group.
+struct GroupBox {
+  float cx, cy, cz, hx, hy, hz;
+  float reach2;
+};
+
+// Particle sources of the batch wl.pp[0..m): each lane loads one source,
+// drops it if it lies beyond the group's reach (it would add nothing to any
+// lane), and the kept ones are compacted, in order, into wl.stage; then every
+// lane evaluates every kept source against its target.
+TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpi, float cpu,
+                   const GroupBox &gb, float rs2, const float2 *__restrict__ t0, float wmax,
+                   unsigned long long &npp) {
   int lane = threadIdx.x & 31;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
   // all loads of the batch are issued before any is used
   uint32_t u[kPpBatch / 32][3];
 #pragma unroll
@@ -528,13 +542,25 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
       u[b][2] = spos[3 * (int64_t)idx + 2];
     }
   }
+  int kept = 0;
 #pragma unroll
   for (int b = 0; b < kPpBatch / 32; b++) {
     int k = b * 32 + lane;
-    if (k < m)
-      wl.stage[k] = make_float4(wrapf(u[b][0], w.rx, cpi), wrapf(u[b][1], w.ry, cpi), wrapf(u[b][2], w.rz, cpi), 0.f);
+    bool keep = false;
+    if (k < m) {
+      float dx = fmaxf(fabsf(wrapf(u[b][0], w.rx, cpu) - gb.cx) - gb.hx, 0.f);
+      float dy = fmaxf(fabsf(wrapf(u[b][1], w.ry, cpu) - gb.cy) - gb.hy, 0.f);
+      float dz = fmaxf(fabsf(wrapf(u[b][2], w.rz, cpu) - gb.cz) - gb.hz, 0.f);
+      keep = dx * dx + dy * dy + dz * dz <= gb.reach2;
+    }
+    unsigned mk = __ballot_sync(0xffffffffu, keep);
+    if (keep)
+      wl.stage[kept + __popc(mk & lanemask_lt)] =
+          make_float4(wrapf(u[b][0], w.rx, cpi), wrapf(u[b][1], w.ry, cpi), wrapf(u[b][2], w.rz, cpi), 0.f);
+    kept += __popc(mk);
   }
   __syncwarp();
+  m = kept;
   float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
   float a2x = 0.f, a2y = 0.f, a2z = 0.f, a3x = 0.f, a3y = 0.f, a3z = 0.f;
   int j = 0;
@@ -682,6 +708,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     float hx = 0.5f * (hix - lox), hy = 0.5f * (hiy - loy), hz = 0.5f * (hiz - loz);
     // a little slack against float rounding of the relative coordinates
     float rs2_prune = rs2 * 1.0001f + 1e-4f;
+    const GroupBox gbox{cx, cy, cz, hx, hy, hz, rs2_prune};
     int top = 0, npcl = 0, nppl = 0;
     if (lane == 0) stack.put(0, 0u);
     top = 1;
@@ -778,7 +805,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
           c -= take2;
           __syncwarp();
           if (nppl == kPpBatch) {
-            eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
+            eval_pp(wl, nppl, spos, w, cpi, cpu, gbox, rs2i, t0, wmax, npp);
             nppl = 0;
           }
         }
@@ -789,7 +816,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
       continue;
     }
     if (npcl > 0) eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, g12, delta, wmax, npc);
-    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpi, rs2i, t0, wmax, npp);
+    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpi, cpu, gbox, rs2i, t0, wmax, npp);
     if (w.active) {
       // the particle sums used separations in index units: back to cells
       int64_t i = (int64_t)gs + lane;

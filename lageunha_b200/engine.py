@@ -59,6 +59,21 @@ def cosmology(omep=0.26, omeplam=0.74, wlam0=-1.0, wlam1=0.0, amax=48.0) -> TpmC
     return TpmCosmology(omep, omeplam, wlam0, wlam1, amax)
 
 
+class TpmRequest(ctypes.Structure):
+    _fields_ = [("params", TpmParams), ("np", ctypes.c_int64), ("pos", ctypes.c_void_p), ("vel", ctypes.c_void_p),
+                ("cosmo", TpmCosmology), ("anow", ctypes.c_float), ("astep", ctypes.c_float),
+                ("nsteps", ctypes.c_int32), ("pos_out", ctypes.c_void_p), ("vel_out", ctypes.c_void_p),
+                ("force_out", ctypes.c_void_p)]
+
+
+class TpmRequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int32), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double), ("device_bytes", ctypes.c_int64)]
+
+
+REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
 class EngineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"tpm error {code}: {msg}")
@@ -106,6 +121,13 @@ _SIGS = {
     "tpm_batch_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.POINTER(ctypes.c_float),
                                       ctypes.POINTER(ctypes.c_float)]),
     "tpm_batch_time": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float)]),
+    "tpm_estimate_bytes": (ctypes.c_int64, [ctypes.c_int32, ctypes.c_int64]),
+    "tpm_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "tpm_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(TpmRequest), ctypes.POINTER(ctypes.c_int64)]),
+    "tpm_server_info": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(TpmRequestInfo)]),
+    "tpm_server_wait": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double]),
+    "tpm_server_stats": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_server_destroy": (ctypes.c_int, [_P]),
     "tpm_evol_factors": (ctypes.c_int, [ctypes.POINTER(TpmCosmology), ctypes.c_int32, ctypes.c_float,
                                         ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
     "tpm_hubble_drag": (ctypes.c_int, [_P, ctypes.c_float]),
@@ -373,6 +395,83 @@ class Batch:
         ms = ctypes.c_float()
         _check(self._lib.tpm_batch_time(self._b, ctypes.byref(ms)))
         return ms.value
+
+
+SERVER_STATS = ("done", "failed", "peak_active", "peak_bytes", "contexts_created", "contexts_reused",
+                "contexts_evicted", "deferred_admissions")
+
+
+def estimate_bytes(n_mesh: int, np_: int) -> int:
+    return int(load_library().tpm_estimate_bytes(n_mesh, np_))
+
+
+class Server:
+    """The request loop (tpm_server_*): continuous batching of force and step
+    requests for boxes of different sizes on one device. Arrays handed to
+    submit() are kept referenced here until the server is closed."""
+
+    def __init__(self, hbm_cap_bytes: int = 150 * 10 ** 9, max_active: int = 64, device: int = 0):
+        self._lib = load_library()
+        s = ctypes.c_void_p()
+        _check(self._lib.tpm_server_create(device, int(hbm_cap_bytes), max_active, ctypes.byref(s)))
+        self._s = s
+        self._keep = {}
+
+    def submit(self, pos, vel=None, *, n_mesh: int, nsteps: int = 0, anow: float = 1.0, astep: float = 0.0,
+               cosmo: TpmCosmology | None = None, pos_out=None, vel_out=None, force_out=None, **params) -> int:
+        p = default_params(n_mesh)
+        for k, v in params.items():
+            if k == "law":
+                v = {"reference": TPM_LAW_REFERENCE, "gaussian": TPM_LAW_GAUSSIAN}.get(v, v)
+            setattr(p, k, v)
+        pos = np.ascontiguousarray(pos, np.uint32)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float32)
+        r = TpmRequest()
+        r.params = p
+        r.np = pos.shape[0]
+        r.pos = pos.ctypes.data
+        r.vel = None if vel is None else vel.ctypes.data
+        r.cosmo = cosmo if cosmo is not None else cosmology()
+        r.anow, r.astep, r.nsteps = anow, astep, nsteps
+        for name, arr in (("pos_out", pos_out), ("vel_out", vel_out), ("force_out", force_out)):
+            if arr is not None:
+                assert arr.flags["C_CONTIGUOUS"] and arr.shape == (r.np, 3) and arr.itemsize == 4
+                setattr(r, name, arr.ctypes.data)
+        rid = ctypes.c_int64()
+        _check(self._lib.tpm_server_submit(self._s, ctypes.byref(r), ctypes.byref(rid)))
+        self._keep[rid.value] = (pos, vel, pos_out, vel_out, force_out)
+        return rid.value
+
+    def info(self, rid: int) -> TpmRequestInfo:
+        out = TpmRequestInfo()
+        _check(self._lib.tpm_server_info(self._s, rid, ctypes.byref(out)))
+        return out
+
+    def wait(self, rid: int = -1, timeout: float = 600.0):
+        _check(self._lib.tpm_server_wait(self._s, rid, timeout))
+
+    def stats(self) -> dict:
+        out = np.zeros(8, np.int64)
+        k = self._lib.tpm_server_stats(self._s, out.ctypes.data, 8)
+        return {SERVER_STATS[i]: int(out[i]) for i in range(k)}
+
+    def close(self):
+        if self._s:
+            self._lib.tpm_server_destroy(self._s)
+            self._s = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def evol_factors(cosmo: TpmCosmology, nx: int, anow: float, astep: float) -> dict:
