@@ -112,8 +112,12 @@ def _ncu_traffic():
     try:
         for line in open(os.path.join(ROOT, "profiles", "ncu_traffic.txt")):
             p = line.split()
-            if len(p) >= 3 and not line.startswith("#"):
-                out[p[0]] = (float(p[1]), float(p[2]))
+            if len(p) < 3 or line.startswith("#"):
+                continue
+            try:
+                out[p[0]] = (float(p[-2]), float(p[-1]))
+            except ValueError:
+                continue
     except OSError:
         pass
     return out

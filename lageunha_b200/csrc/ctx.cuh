@@ -64,6 +64,8 @@ struct tpm_ctx {
   float2 *spec2 = nullptr;
   float *phi2 = nullptr;
   CUtensorMap tmap4b;
+  float *gt = nullptr;       // tabulated influence function of the pair
+  float gt_rs = -1.f;        // split scale gt was computed for
   uint32_t *tile_start = nullptr;
   // tree
   tpm::TreeBuffers tb;

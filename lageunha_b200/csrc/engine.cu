@@ -185,15 +185,32 @@ static void free_mesh2(tpm_ctx *c) {
   if (c->rho2) cudaFree(c->rho2);
   if (c->spec2) cudaFree(c->spec2);
   if (c->phi2) cudaFree(c->phi2);
+  if (c->gt) cudaFree(c->gt);
   c->rho2 = nullptr;
   c->spec2 = nullptr;
   c->phi2 = nullptr;
+  c->gt = nullptr;
+  c->gt_rs = -1.f;
 }
 
-// The second (half-cell-shifted) grid of the Gaussian law's interlaced PM.
+// The second (half-cell-shifted) grid of the Gaussian law's interlaced PM and
+// the pair's influence function for the current split scale.
 static int ensure_mesh2(tpm_ctx *c) {
-  if (c->prm.law != TPM_LAW_GAUSSIAN || c->rho2) return 0;
+  if (c->prm.law != TPM_LAW_GAUSSIAN) return 0;
   const MeshGeom &g = c->g;
+  if (c->rho2) {
+    if (c->gt_rs != c->prm.rs_split) {
+      launch_green_opt(c->gt, g.n, (double)c->prm.rs_split, c->st);
+      CK(cudaGetLastError());
+      c->gt_rs = c->prm.rs_split;
+      c->gen++;
+    }
+    return 0;
+  }
+  CK(cudaMalloc(&c->gt, sizeof(float) * (int64_t)g.n * g.hx * g.n));
+  launch_green_opt(c->gt, g.n, (double)c->prm.rs_split, c->st);
+  CK(cudaGetLastError());
+  c->gt_rs = c->prm.rs_split;
   int64_t n3 = (int64_t)g.n * g.n * g.n;
   CK(cudaMalloc(&c->rho2, sizeof(float) * n3));
   CK(cudaMalloc(&c->spec2, sizeof(float2) * g.spec_elems));
@@ -433,7 +450,7 @@ int64_t tpm::ctx_bytes(int n_mesh, int64_t np) {
   MeshGeom g = make_geom(n_mesh);
   int64_t n3 = (int64_t)g.n * g.n * g.n;
   // both grids of the interlaced pair (the Gaussian law's second grid)
-  int64_t mesh = 2 * (4 * n3 + 8 * g.spec_elems + 4 * (int64_t)g.px * g.py * g.pz);
+  int64_t mesh = 2 * (4 * n3 + 8 * g.spec_elems + 4 * (int64_t)g.px * g.py * g.pz) + 4 * g.spec_elems;
   int64_t ntiles = 1ll << (3 * (g.cbits - 3)), ncubes = 1ll << (3 * (g.cbits - 2));
   mesh += 4 * (ntiles + 1) + 4 * (ncubes + 1) + 8 * (int64_t)(n_mesh + n_mesh / 2 + 1);
   int64_t parts = np * (12 + 12 + 8 + 8 + 4 + 4 + 12 + 12 + 12 + 12) + 4 * 256 * (sort_tiles(np) + 1) + 1024;
@@ -667,7 +684,7 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     if (timing) CK(cudaEventRecord(c->ev[2], st));
     if (il)
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
-                     &c->launches, c->rho2, c->spec2, c->phi2);
+                     &c->launches, c->rho2, c->spec2, c->phi2, c->gt);
     else
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
                      &c->launches);

@@ -75,7 +75,10 @@ void fft_plan_free(FftPlan &p);
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
                     int64_t *launches, const float *rho2 = nullptr, float2 *spec2 = nullptr,
-                    float *phi2_pad = nullptr);
+                    float *phi2_pad = nullptr, const float *gt = nullptr);
+// The optimal influence function of the interlaced pair with the 8-point
+// gradient for split scale rs, [ky][kx][kz] with kx < n/2 + 1.
+void launch_green_opt(float *gt, int n, double rs, cudaStream_t st);
 // fda4: gradient and TSC interpolation per tile through TMA.
 // half: positions moved by half a cell (the shifted grid); average: write the
 // mean of the new force and the one already in fpm.

@@ -13,6 +13,8 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
+
 #include "engine_internal.cuh"
 
 namespace tpm {
@@ -470,6 +472,7 @@ struct GreenArgs {
   float irngc;   // 1 / n^3
   float rs2k;    // gaussian law: (2 pi rs / n)^2
   int n;
+  const float *gt;  // tabulated influence function [ky][kx][kz] (interlaced grids), or null
 };
 
 TPM_D float green(const GreenArgs &g, int kx, int ky, int kz) {
@@ -541,7 +544,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
       for (int e = tid; e < TX * L; e += nth) {
         int q = e / L, m = e - q * L;
         int kx = kx0 + q, wz = m > n / 2 ? m - n : m;
-        float gk = green(ga, kx, outer, m);
+        float gk = ga.gt ? ga.gt[((int64_t)outer * hx + kx) * n + m] : green(ga, kx, outer, m);
         if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
         float s, c;
         sincospif((float)(kx + wy + wz) / (float)n, &s, &c);
@@ -655,9 +658,70 @@ static int cols_per_block(int n, int hx, int nspec) {
   return TX;
 }
 
+// The optimal influence function of the interlaced TSC pair with the 8-point
+// gradient (Hockney & Eastwood, "Computer Simulation Using Particles", ch. 8;
+// interlaced form after Neelov & Holm 2010): the Green's function that
+// minimises the mean-square force error against the Gaussian-filtered
+// reference force R(k) = -i k (-4 pi / k^2) exp(-k^2 rs^2), given the
+// assignment window U and the difference operator D,
+//   G(k) = sum_m U^2(k_m) R(k_m).D(k) / (|D(k)|^2 (sum_m U^2(k_m))^2),
+// k_m = k + 2 pi m, over the alias images m in [-2, 2]^3 that survive
+// interlacing (even m_x + m_y + m_z). In the reference's units (mode numbers,
+// -1/(pi m^2), 1/n^3). Computed once per mesh and split scale, in FP64.
+__global__ void k_green_opt(float *__restrict__ gt, int n, int hx, double rs, double irngc) {
+  const double PI = 3.14159265358979323846;
+  const double c[4] = {4.0 / 5.0, -1.0 / 5.0, 4.0 / 105.0, -1.0 / 280.0};
+  int64_t total = (int64_t)n * hx * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int kz = (int)(i % n);
+    int kx = (int)((i / n) % hx);
+    int ky = (int)(i / ((int64_t)n * hx));
+    int my = ky > n / 2 ? ky - n : ky, mz = kz > n / 2 ? kz - n : kz, mx = kx;
+    float out = 0.f;
+    bool nyq = (n % 2 == 0) && (2 * mx == n || 2 * my == n || 2 * mz == n || -2 * my == n || -2 * mz == n);
+    if (!nyq && (mx | my | mz) != 0) {
+      double k[3] = {2 * PI * mx / n, 2 * PI * my / n, 2 * PI * mz / n};
+      double D[3];
+      for (int a = 0; a < 3; a++) {
+        D[a] = 0;
+        for (int j = 0; j < 4; j++) D[a] += 2 * c[j] * sin((j + 1) * k[a]);
+      }
+      double D2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2];
+      double num = 0, den = 0;
+      for (int ax = -2; ax <= 2; ax++)
+        for (int ay = -2; ay <= 2; ay++)
+          for (int az = -2; az <= 2; az++) {
+            if (((ax + ay + az) & 1) != 0) continue;
+            double q[3] = {k[0] + 2 * PI * ax, k[1] + 2 * PI * ay, k[2] + 2 * PI * az};
+            double U2 = 1;
+            for (int a = 0; a < 3; a++) {
+              double h = 0.5 * q[a];
+              double s = h == 0 ? 1.0 : sin(h) / h;
+              double s3 = s * s * s;
+              U2 *= s3 * s3;
+            }
+            double q2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            double m2 = q2 * (n / (2 * PI)) * (n / (2 * PI));
+            double Rs = -1.0 / PI / m2 * exp(-q2 * rs * rs);
+            num += U2 * Rs * (D[0] * q[0] + D[1] * q[1] + D[2] * q[2]);
+            den += U2;
+          }
+      if (D2 > 0 && den > 0) out = (float)(num / (D2 * den * den) * irngc);
+    }
+    gt[i] = out;
+  }
+}
+
+void launch_green_opt(float *gt, int n, double rs, cudaStream_t st) {
+  int hx = n / 2 + 1;
+  int64_t total = (int64_t)n * hx * n;
+  int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  k_green_opt<<<blocks, 256, 0, st>>>(gt, n, hx, rs, 1.0 / ((double)n * n * n));
+}
+
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
-                    int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad) {
+                    int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad, const float *gt) {
   int n = g.n;
   int64_t nrows = (int64_t)n * n;
   bool packed = (n % 2) == 0;
@@ -681,6 +745,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   ga.sfact = (float)(-pow(M_PI * (double)efold / (double)n, 2));
   ga.irngc = (float)(1.0 / ((double)n * n * n));
   ga.rs2k = (float)pow(2.0 * M_PI * (double)rs_split / (double)n, 2);
+  ga.gt = rho2 ? gt : nullptr;
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, -1.f, 0, ga, TX, nspec);
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 2, -1.f, 1, ga, TX, nspec);
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, 1.f, 0, ga, TX, nspec);
