@@ -208,6 +208,29 @@ int tpm_batch_step(tpm_batch *batch, const tpm_cosmology *cosmo, const float *an
 /* Device time of the last tpm_batch_compute / tpm_batch_step launch, ms. */
 int tpm_batch_time(tpm_batch *batch, float *ms);
 
+/* ---- the autotuner ---- */
+
+/* Launch shapes picked by timing candidates on the context's loaded
+ * particles (each three times, median). TPM_TUNE_FFT: pencils per block of
+ * the x transforms and kx columns per block of the y/z transforms (forces do
+ * not change). TPM_TUNE_GROUPS: targets per warp group (16 or 32) and the
+ * cube the groups are cut from (2^group_level cells, 4 or 8); the tree force
+ * changes within its error, since a group opens a node if any target would.
+ * The choice stays in the context; tpm_set_tuning applies it to other boxes
+ * of the same size. 0 in fft_* means the built-in shape. No counterpart in the
+ * reference. */
+#define TPM_TUNE_FFT 1u
+#define TPM_TUNE_GROUPS 2u
+typedef struct tpm_tuning {
+  int32_t fft_pencils_x, fft_cols;
+  int32_t group_level, group_max;
+  float ms_fft, ms_fft_default;    /* the chosen and the built-in shape, ms */
+  float ms_walk, ms_walk_default;  /* groups + walk, chosen and built-in, ms */
+} tpm_tuning;
+int tpm_autotune(tpm_ctx *ctx, unsigned what, tpm_tuning *out);
+int tpm_get_tuning(const tpm_ctx *ctx, tpm_tuning *out);
+int tpm_set_tuning(tpm_ctx *ctx, const tpm_tuning *tuning);
+
 /* ---- the request loop (served solves) ---- */
 
 /* A worker thread on one device admits requests in arrival order while

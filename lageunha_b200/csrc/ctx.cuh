@@ -76,6 +76,10 @@ struct tpm_ctx {
   float law_eps = -1, law_rs = -1, law_rsphere = -1;
   int law_kind = -1;
   uint32_t *err = nullptr;
+  // launch shapes (tpm_autotune): 0 = the built-in choice
+  int tune_fft_px = 0, tune_fft_tx = 0;
+  int tune_group_level = 2;  // groups live in cubes of 2^level cells
+  int tune_group_max = 32;   // targets per warp group
   // graphs: gen counts every change of buffers or parameters baked into a
   // captured launch; herr/hfac are pinned host words the graphs copy through
   uint64_t gen = 1;
@@ -105,8 +109,12 @@ const std::string &last_error_string();
   } while (0)
 
 // Enqueues one force evaluation of the loaded particles on st (no host
-// synchronisation); with timing, records the stage events.
-int enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing);
+// synchronisation); with timing, records the stage events. walk == false
+// stops before the tree walk (the tree and the groups are built): an
+// ensemble walks all its boxes in one launch.
+int enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing, bool walk = true);
+// The walk record of the context's current buffers.
+WalkBox ctx_walk_box(const tpm_ctx *c);
 // After the stream has finished an evaluation: checks the device error words
 // (from c->err, or from the pinned copy when from_host), and on success marks
 // the parts valid and reads the tree counters.

@@ -127,7 +127,9 @@ static int build_law(tpm_ctx *c) {
   const double range = 6.0;
   float ran2nran = (float)(range / NS);
   float invran = (float)(1.0 / ran2nran);
-  double LL = (double)p.n_mesh * (double)p.n_mesh;
+  // the table is per unit LL (= N^2): the walk scales each box's forces by
+  // its own 1/N^2, so boxes of every mesh size share one table
+  double LL = 1.0;
   double dr = ran2nran * 0.1;
   std::vector<double> diff((NS + 1) * 3, 0.0), slope(NS * 3, 0.0);
   for (int i = 1; i < NS; i++) {
@@ -159,6 +161,18 @@ static int build_law(tpm_ctx *c) {
                          (float)(slope[3 * i + 2] * dl));
   }
   t0[entries] = make_float2(0.f, 0.f);
+  int hard_cut = 1;
+  if (p.law == TPM_LAW_GAUSSIAN) {
+    // the particle-particle column falls to zero at the first node kc at or
+    // beyond the cut: the pair term ramps to zero over the last interval
+    // (width 6/4096 cells) instead of stopping at r = rsphere exactly
+    int kc = (int)ceil((double)p.rsphere * invran);
+    if (kc >= 1 && kc < entries) {
+      for (int i = kc; i <= entries; i++) t0[i] = make_float2(0.f, 0.f);
+      t0[kc - 1].y = -t0[kc - 1].x;
+      hard_cut = 0;
+    }
+  }
   if (c->law.t0 || c->law.t12) CK(cudaStreamSynchronize(c->st));
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
@@ -169,6 +183,7 @@ static int build_law(tpm_ctx *c) {
   CK(cudaMemcpy(c->law.t0, t0.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->law.t12, t12.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
   c->law.entries = entries;
+  c->law.hard_cut = hard_cut;
   c->law.delta = ran2nran;
   c->law.inv_delta = invran;
   c->law_n = p.n_mesh;
@@ -445,6 +460,17 @@ int tpm::launch_finish(tpm_ctx *c, cudaStream_t st) {
   return 0;
 }
 
+WalkBox tpm::ctx_walk_box(const tpm_ctx *c) {
+  TreeParams tp;
+  tp.n = (uint32_t)c->g.n;
+  tp.sub_bits = c->g.sub_bits;
+  tp.theta2 = c->prm.theta * c->prm.theta;
+  tp.rsphere = c->prm.rsphere;
+  tp.cell_per_unit = (float)((double)c->g.n / 4294967296.0);
+  tp.mass = c->prm.particle_mass;
+  return walk_box(tp, c->spos, c->tb, c->law, c->ftree, c->err);
+}
+
 int64_t tpm::ctx_bytes(int n_mesh, int64_t np) {
   // the allocations of tpm_create, alloc_mesh and ensure_particles
   MeshGeom g = make_geom(n_mesh);
@@ -508,7 +534,8 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
   // the allocations below are mirrored by ctx_bytes()
   if (cudaMalloc(&c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
       cudaMalloc(&c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
-      cudaMalloc(&c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess) {
+      cudaMalloc(&c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess ||
+      cudaMalloc(&c->tb.walkbox, sizeof(WalkBox)) != cudaSuccess) {
     tpm_destroy(c);
     return fail(TPM_E_NOMEM, "cudaMalloc of context scratch failed");
   }
@@ -549,6 +576,7 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->err) cudaFree(c->err);
   if (c->tb.counters) cudaFree(c->tb.counters);
   if (c->tb.level_range) cudaFree(c->tb.level_range);
+  if (c->tb.walkbox) cudaFree(c->tb.walkbox);
   if (c->tb.stack) cudaFree(c->tb.stack);
   if (c->stage) cudaFree(c->stage);
   for (CapturedGraph &gr : c->graphs) {
@@ -648,7 +676,7 @@ int tpm_load_lagrangian(tpm_ctx *c, int64_t np, const void *particles, int64_t s
 
 }  // extern "C"
 
-int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing) {
+int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing, bool walk) {
   const MeshGeom &g = c->g;
   int64_t np = c->np;
   c->launches = 0;
@@ -684,10 +712,10 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     if (timing) CK(cudaEventRecord(c->ev[2], st));
     if (il)
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
-                     &c->launches, c->rho2, c->spec2, c->phi2, c->gt);
+                     &c->launches, c->rho2, c->spec2, c->phi2, c->gt, c->tune_fft_px, c->tune_fft_tx);
     else
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
-                     &c->launches);
+                     &c->launches, nullptr, nullptr, nullptr, nullptr, c->tune_fft_px, c->tune_fft_tx);
     CK(stage_check(st, "fft"));
     if (timing) CK(cudaEventRecord(c->ev[3], st));
     // the reference law keeps the reference's 4-point gradient; the Gaussian
@@ -714,12 +742,15 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     tp.rsphere = c->prm.rsphere;
     tp.cell_per_unit = (float)((double)g.n / 4294967296.0);
     tp.mass = c->prm.particle_mass;
+    tp.group_max = c->tune_group_max;
     tree_build(tp, c->skey, c->spos, np, c->tb, c->err, st, &c->launches);
     CK(cudaMemsetAsync(c->tb.counters, 0, sizeof(uint32_t) * 16, st));
-    tree_groups(tp, c->skey, np, c->tb, c->cube_start, c->ncubes, 3 * (g.sub_bits + 2), st, &c->launches);
+    int glev = c->tune_group_level;
+    int64_t gcubes = 1ll << (3 * (g.cbits - glev));
+    tree_groups(tp, c->skey, np, c->tb, c->cube_start, gcubes, 3 * (g.sub_bits + glev), st, &c->launches);
     CK(stage_check(st, "tree_build"));
     if (timing) CK(cudaEventRecord(c->ev[5], st));
-    tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
+    if (walk) tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
     CK(stage_check(st, "tree_walk"));
     if (timing) CK(cudaEventRecord(c->ev[6], st));
   } else if (timing) {

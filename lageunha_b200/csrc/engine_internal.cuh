@@ -75,7 +75,7 @@ void fft_plan_free(FftPlan &p);
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
                     int64_t *launches, const float *rho2 = nullptr, float2 *spec2 = nullptr,
-                    float *phi2_pad = nullptr, const float *gt = nullptr);
+                    float *phi2_pad = nullptr, const float *gt = nullptr, int want_px = 0, int want_tx = 0);
 // The optimal influence function of the interlaced pair with the 8-point
 // gradient for split scale rs, [ky][kx][kz] with kx < n/2 + 1.
 void launch_green_opt(float *gt, int n, double rs, cudaStream_t st);
@@ -90,6 +90,17 @@ void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const u
 int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorMap *out);
 
 // ---------------------------------------------------------------- tree
+// What the walk reads of one box (the ensemble walk holds an array of them).
+struct WalkBox {
+  const uint32_t *spos;
+  const uint4 *walkA, *walkB;
+  const float4 *mom0, *mom1, *mom2;
+  const uint32_t *groups;
+  const uint32_t *ngroups;  // device word: the box's group count
+  float *ftree;
+  uint32_t *err;
+  float cpu, cpi, mass, inv_ll;
+};
 struct TreeBuffers {
   int64_t cap_nodes = 0;
   uint32_t *start = nullptr, *count = nullptr, *child = nullptr, *nchild = nullptr;
@@ -111,6 +122,7 @@ struct TreeBuffers {
   uint32_t *counters = nullptr;     // [8]: ngroups, next group, pp, pc, ...
   uint32_t *stack = nullptr;        // per-warp global stacks
   int64_t stack_words = 0;
+  WalkBox *walkbox = nullptr;       // device copy of this box's walk record
 };
 
 struct TreeParams {
@@ -120,6 +132,7 @@ struct TreeParams {
   float rsphere;
   float cell_per_unit;  // n / 2^32
   float mass;
+  int group_max = 32;   // targets per warp group (<= 32)
 };
 
 void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos, int64_t np,
@@ -136,7 +149,16 @@ struct LawTable {
   float4 *t12 = nullptr;
   int entries = 0;
   float delta = 0, inv_delta = 0;
+  // 1: the walk tests r <= rsphere per pair (the reference's cut);
+  // 0: t0 is zero from the cut on, so the pair test is not needed
+  int hard_cut = 1;
 };
+WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, const LawTable &law,
+                 float *ftree, uint32_t *err);
+// One launch over the groups of every box (boxes: device array); the boxes
+// share law (same kind, softening, split and cut) and rsphere.
+void tree_walk_multi(const WalkBox *boxes, int nbox, uint32_t *gprefix, uint32_t *gnext, uint32_t *stack,
+                     int64_t stack_words, uint32_t *stats, const LawTable &law, float rsphere, cudaStream_t st);
 void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
                const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st,
                int64_t *launches);

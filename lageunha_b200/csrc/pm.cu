@@ -639,7 +639,12 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
   }
 }
 
-static int pencils_for(int L) {
+static int pencils_for(int L, int want = 0) {
+  if (want > 0) {
+    // a tuned count, kept within the 160 KB of shared memory
+    int cap = (int)(((160 * 1024) / (int)sizeof(float2) - L) / (2 * L));
+    return std::max(1, std::min(want, cap));
+  }
   int P = 4096 / L;
   if (P < 1) P = 1;
   if (P > 64) P = 64;
@@ -649,8 +654,8 @@ static int pencils_for(int L) {
 // Columns per block of the y and z passes: 8 (16 below n = 256) consecutive
 // kx, fewer where the block's shared memory (twiddles + two buffers of
 // nspec * TX pencils) would exceed 160 KB.
-static int cols_per_block(int n, int hx, int nspec) {
-  int TX = n >= 256 ? 8 : 16;
+static int cols_per_block(int n, int hx, int nspec, int want = 0) {
+  int TX = want > 0 ? want : (n >= 256 ? 8 : 16);
   int tmax = (int)(((160 * 1024) / (int)sizeof(float2) / n - 1) / (2 * nspec));
   if (TX > tmax) TX = tmax;
   if (TX > hx) TX = hx;
@@ -721,12 +726,13 @@ void launch_green_opt(float *gt, int n, double rs, cudaStream_t st) {
 
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
-                    int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad, const float *gt) {
+                    int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad, const float *gt,
+                    int want_px, int want_tx) {
   int n = g.n;
   int64_t nrows = (int64_t)n * n;
   bool packed = (n % 2) == 0;
   int Lx = packed ? n / 2 : n;
-  int Px = pencils_for(Lx);
+  int Px = pencils_for(Lx, want_px);
   FftArgs ax = fft_args(n, Lx, Px);
   const float2 *twL = packed ? p.tw_half : p.tw;
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
@@ -735,7 +741,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho, spec, ax, twL, p.tw, nrows);
   if (rho2) k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho2, spec2, ax, twL, p.tw, nrows);
   // columns
-  int TX = cols_per_block(n, g.hx, nspec);
+  int TX = cols_per_block(n, g.hx, nspec, want_tx);
   FftArgs ac = fft_args(n, n, TX * nspec);
   size_t smc = sizeof(float2) * (n + 2 * TX * nspec * n);
   int ntx = (g.hx + TX - 1) / TX;

@@ -20,6 +20,8 @@
 // coordinates are exact minimum-image differences converted to float.
 #include <stdio.h>
 
+#include <algorithm>
+
 #include "engine_internal.cuh"
 
 namespace tpm {
@@ -340,11 +342,11 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
 // ------------------------------------------------------------ walk groups
 // Groups never cross a 4-cell cube and hold at most 32 particles.
 __global__ void k_group_counts(const uint32_t *__restrict__ cube_start, int64_t ncubes,
-                               uint32_t *__restrict__ gcount) {
+                               uint32_t *__restrict__ gcount, uint32_t gmax) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncubes;
        c += (int64_t)gridDim.x * blockDim.x) {
     uint32_t cnt = cube_start[c + 1] - cube_start[c];
-    gcount[c] = (cnt + 31) / 32;
+    gcount[c] = (cnt + gmax - 1) / gmax;
   }
 }
 
@@ -421,14 +423,14 @@ __global__ void __launch_bounds__(1024) k_scan_sums(uint32_t *bsum, int64_t nb, 
 
 __global__ void k_write_groups(const uint32_t *__restrict__ cube_start, int64_t ncubes,
                                const uint32_t *__restrict__ goff, const uint32_t *__restrict__ bsum,
-                               uint32_t *__restrict__ groups) {
+                               uint32_t *__restrict__ groups, uint32_t gmax) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncubes;
        c += (int64_t)gridDim.x * blockDim.x) {
     uint32_t s = cube_start[c], e = cube_start[c + 1];
     uint32_t g = goff[c] + bsum[c / 4096];
-    for (uint32_t p = s; p < e; p += 32, g++) {
+    for (uint32_t p = s; p < e; p += gmax, g++) {
       groups[2 * (int64_t)g] = p;
-      groups[2 * (int64_t)g + 1] = min(32u, e - p);
+      groups[2 * (int64_t)g + 1] = min(gmax, e - p);
     }
   }
 }
@@ -436,7 +438,7 @@ __global__ void k_write_groups(const uint32_t *__restrict__ cube_start, int64_t 
 void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
                  uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
                  int64_t *launches) {
-  (void)tp;
+  uint32_t gmax = (uint32_t)std::max(1, std::min(32, tp.group_max));
   launch_range_table(key, np, cube_shift, (uint32_t)ncubes, cube_start, st);
   // gcount and offsets live in the tail of the group buffer's scratch
   uint32_t *gcount = tb.tile_sum;  // sized >= ncubes + blocks by the caller
@@ -445,10 +447,10 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
   uint32_t *bsum = goff + ncubes;
   int blocks = (int)((ncubes + 255) / 256);
   if (blocks > 148 * 16) blocks = 148 * 16;
-  k_group_counts<<<blocks, 256, 0, st>>>(cube_start, ncubes, gcount);
+  k_group_counts<<<blocks, 256, 0, st>>>(cube_start, ncubes, gcount, gmax);
   k_scan_block<<<(unsigned)nb, 1024, 0, st>>>(gcount, goff, ncubes, bsum);
   k_scan_sums<<<1, 1024, 0, st>>>(bsum, nb, &tb.counters[0]);
-  k_write_groups<<<blocks, 256, 0, st>>>(cube_start, ncubes, goff, bsum, tb.groups);
+  k_write_groups<<<blocks, 256, 0, st>>>(cube_start, ncubes, goff, bsum, tb.groups, gmax);
   if (launches) *launches += 5;
 }
 
@@ -461,6 +463,7 @@ constexpr int kPcCap = 64;
 constexpr int kPpBatch = 96;       // particle sources evaluated per flush
 
 struct WarpLists {
+  WalkBox box;                     // the box of the group this warp walks
   uint32_t pc[kPcCap];
   uint32_t pp[kPpBatch];
   float4 stage[kPpBatch];          // PP: one float4 per source; PC: three per node
@@ -498,6 +501,9 @@ TPM_D int table_index(float w, float &frac) {
 // Coordinates are in table-index units (cells / delta); r2 = 0 (the target
 // itself) gives rsqrt = inf, w = NaN, which fminf turns into wmax, and a zero
 // separation, so it adds nothing.
+// kHardCut: the per-pair r^2 <= rsphere^2 test of the reference law; a table
+// that already falls to zero at the cut (the Gaussian law's) needs none.
+template <bool kHardCut>
 TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, const float2 *__restrict__ t0,
                    float &ax, float &ay, float &az) {
   float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
@@ -507,7 +513,7 @@ TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, cons
   int nt = table_index(wq, frac);
   float2 c = t0[nt];
   float f = fmaf(c.y, frac, c.x);
-  f = r2 <= rs2 ? f : 0.f;
+  if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
   ay = fmaf(dy, f, ay);
   az = fmaf(dz, f, az);
@@ -525,6 +531,7 @@ struct GroupBox {
 // drops it if it lies beyond the group's reach (it would add nothing to any
 // lane), and the kept ones are compacted, in order, into wl.stage; then every
 // lane evaluates every kept source against its target.
+template <bool kHardCut>
 TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpi, float cpu,
                    const GroupBox &gb, float rs2, const float2 *__restrict__ t0, float wmax,
                    unsigned long long &npp) {
@@ -565,12 +572,12 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
   float a2x = 0.f, a2y = 0.f, a2z = 0.f, a3x = 0.f, a3y = 0.f, a3z = 0.f;
   int j = 0;
   for (; j + 4 <= m; j += 4) {
-    pp_body(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
-    pp_body(wl.stage[j + 1], w, rs2, wmax, t0, a1x, a1y, a1z);
-    pp_body(wl.stage[j + 2], w, rs2, wmax, t0, a2x, a2y, a2z);
-    pp_body(wl.stage[j + 3], w, rs2, wmax, t0, a3x, a3y, a3z);
+    pp_body<kHardCut>(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
+    pp_body<kHardCut>(wl.stage[j + 1], w, rs2, wmax, t0, a1x, a1y, a1z);
+    pp_body<kHardCut>(wl.stage[j + 2], w, rs2, wmax, t0, a2x, a2y, a2z);
+    pp_body<kHardCut>(wl.stage[j + 3], w, rs2, wmax, t0, a3x, a3y, a3z);
   }
-  for (; j < m; j++) pp_body(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
+  for (; j < m; j++) pp_body<kHardCut>(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
   if (w.active) {
     w.ax += (a0x + a1x) + (a2x + a3x);
     w.ay += (a0y + a1y) + (a2y + a3y);
@@ -583,7 +590,7 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 // Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
 // and z components on their own axes. Coordinates are in table-index units;
 // the separations are rescaled to cells with delta for the force terms.
-TPM_D void eval_pc(WarpLists &wl, int m_all, const TreeBuffers &tb, WalkCtx &w, float cpi, float rs2,
+TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpi, float rs2,
                    const float2 *__restrict__ t0, const float4 *__restrict__ t12, float delta,
                    float wmax, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
@@ -647,12 +654,15 @@ struct WarpStack {
   }
 };
 
+// One launch walks the groups of one box (nbox == 1) or of an ensemble
+// (boxes[0..nbox), group g of the launch belonging to the box b with
+// gprefix[b] <= g < gprefix[b+1]). The boxes share the law table, which is
+// per unit LL: each box's forces are scaled by its 1/N^2 at the end.
+template <bool kHardCut>
 __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
-    const uint32_t *__restrict__ spos, TreeBuffers tb, const float2 *__restrict__ g0,
-    const float4 *__restrict__ g12, int entries, float inv_delta, float cpu, float rs2, float mass,
-    float *__restrict__ ftree, uint32_t *__restrict__ err) {
-  // positions relative to the group reference in table-index units
-  const float cpi = cpu * inv_delta;
+    const WalkBox *__restrict__ boxes, const uint32_t *__restrict__ gprefix, int nbox,
+    uint32_t *__restrict__ gnext, uint32_t *__restrict__ stack_base, uint32_t *__restrict__ stats,
+    const float2 *__restrict__ g0, const float4 *__restrict__ g12, int entries, float inv_delta, float rs2) {
   const float rs2i = rs2 * inv_delta * inv_delta;
   const float delta = 1.f / inv_delta;
   extern __shared__ float4 smem4[];
@@ -664,37 +674,62 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
   int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpLists &wl = lists[wib];
   int64_t gwarp = (int64_t)blockIdx.x * kWalkWarps + wib;
-  WarpStack stack{wl.stack, tb.stack + gwarp * (kStackCap - kStackSmem)};
-  uint32_t ngroups = tb.counters[0];
+  WarpStack stack{wl.stack, stack_base + gwarp * (kStackCap - kStackSmem)};
+  const uint32_t ngroups = nbox == 1 ? *boxes[0].ngroups : gprefix[nbox];
   unsigned long long npp = 0, npc = 0, niter = 0, nvisit = 0;
   int max_top = 0;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
+  int cur_box = -1;
   while (true) {
     uint32_t g = 0;
-    if (lane == 0) g = atomicAdd(&tb.counters[1], 1u);
+    if (lane == 0) g = atomicAdd(gnext, 1u);
     g = __shfl_sync(0xffffffffu, g, 0);
     if (g >= ngroups) break;
-    uint32_t gs = tb.groups[2 * (int64_t)g], gc = tb.groups[2 * (int64_t)g + 1];
+    int b = 0;
+    if (nbox > 1) {
+      int lo = 0, hi = nbox - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (gprefix[mid] <= g) lo = mid;
+        else hi = mid - 1;
+      }
+      b = lo;
+      g -= gprefix[b];
+    }
+    if (b != cur_box) {
+      // the box record into this warp's shared memory, one word per lane
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(&boxes[b]);
+      constexpr int kWords = (int)(sizeof(WalkBox) / 4);
+      static_assert(kWords <= 32, "box record larger than a warp's load");
+      uint32_t v = lane < kWords ? src[lane] : 0u;
+      __syncwarp();
+      if (lane < kWords) reinterpret_cast<uint32_t *>(&wl.box)[lane] = v;
+      __syncwarp();
+      cur_box = b;
+    }
+    // the box's fields are read from the warp's shared copy where they are
+    // used, which keeps them out of the registers the inner loops need
+    uint32_t gs = wl.box.groups[2 * (int64_t)g], gc = wl.box.groups[2 * (int64_t)g + 1];
     WalkCtx w;
     w.active = (uint32_t)lane < gc;
     uint32_t ux = 0, uy = 0, uz = 0;
     if (w.active) {
-      ux = spos[3 * (int64_t)(gs + lane) + 0];
-      uy = spos[3 * (int64_t)(gs + lane) + 1];
-      uz = spos[3 * (int64_t)(gs + lane) + 2];
+      ux = wl.box.spos[3 * (int64_t)(gs + lane) + 0];
+      uy = wl.box.spos[3 * (int64_t)(gs + lane) + 1];
+      uz = wl.box.spos[3 * (int64_t)(gs + lane) + 2];
     }
     w.rx = __shfl_sync(0xffffffffu, ux, 0);
     w.ry = __shfl_sync(0xffffffffu, uy, 0);
     w.rz = __shfl_sync(0xffffffffu, uz, 0);
-    w.tx = w.active ? wrapf(ux, w.rx, cpi) : 0.f;
-    w.ty = w.active ? wrapf(uy, w.ry, cpi) : 0.f;
-    w.tz = w.active ? wrapf(uz, w.rz, cpi) : 0.f;
+    w.tx = w.active ? wrapf(ux, w.rx, wl.box.cpi) : 0.f;
+    w.ty = w.active ? wrapf(uy, w.ry, wl.box.cpi) : 0.f;
+    w.tz = w.active ? wrapf(uz, w.rz, wl.box.cpi) : 0.f;
     w.ax = w.ay = w.az = 0.f;
     w.bx = w.by = w.bz = 0.f;
     // group box in cells
-    float gx0 = w.active ? wrapf(ux, w.rx, cpu) : 0.f;
-    float gy0 = w.active ? wrapf(uy, w.ry, cpu) : 0.f;
-    float gz0 = w.active ? wrapf(uz, w.rz, cpu) : 0.f;
+    float gx0 = w.active ? wrapf(ux, w.rx, wl.box.cpu) : 0.f;
+    float gy0 = w.active ? wrapf(uy, w.ry, wl.box.cpu) : 0.f;
+    float gz0 = w.active ? wrapf(uz, w.rz, wl.box.cpu) : 0.f;
     float lox = gx0, hix = gx0, loy = gy0, hiy = gy0, loz = gz0, hiz = gz0;
     for (int o = 16; o > 0; o >>= 1) {
       lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
@@ -728,15 +763,15 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
       int kind = 0;  // 0 drop, 1 accept (PC), 2 open (push children), 3 particles (PP)
       uint32_t c0 = 0, nch = 0, ps = 0, pcnt = 0;
       if (has) {
-        uint4 geo = tb.walkA[2 * (int64_t)node];
-        uint4 com = tb.walkA[2 * (int64_t)node + 1];
-        uint4 rec = tb.walkB[node];
+        uint4 geo = wl.box.walkA[2 * (int64_t)node];
+        uint4 com = wl.box.walkA[2 * (int64_t)node + 1];
+        uint4 rec = wl.box.walkB[node];
         int lev = (int)(rec.w >> 16);
         nch = rec.w & 0xffffu;
         float half = __uint_as_float(geo.w);
-        float dx = fmaxf(fabsf(wrapf(geo.x, w.rx, cpu) - cx) - half - hx, 0.f);
-        float dy = fmaxf(fabsf(wrapf(geo.y, w.ry, cpu) - cy) - half - hy, 0.f);
-        float dz = fmaxf(fabsf(wrapf(geo.z, w.rz, cpu) - cz) - half - hz, 0.f);
+        float dx = fmaxf(fabsf(wrapf(geo.x, w.rx, wl.box.cpu) - cx) - half - hx, 0.f);
+        float dy = fmaxf(fabsf(wrapf(geo.y, w.ry, wl.box.cpu) - cy) - half - hy, 0.f);
+        float dz = fmaxf(fabsf(wrapf(geo.z, w.rz, wl.box.cpu) - cz) - half - hz, 0.f);
         bool near = lev < 2 || dx * dx + dy * dy + dz * dz <= rs2_prune;
         if (near) {
           if (lev > 0 && rec.y < (uint32_t)kLeafMin) {
@@ -744,9 +779,9 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
             ps = rec.x;
             pcnt = rec.y;
           } else {
-            float ex = fmaxf(fabsf(wrapf(com.x, w.rx, cpu) - cx) - hx, 0.f);
-            float ey = fmaxf(fabsf(wrapf(com.y, w.ry, cpu) - cy) - hy, 0.f);
-            float ez = fmaxf(fabsf(wrapf(com.z, w.rz, cpu) - cz) - hz, 0.f);
+            float ex = fmaxf(fabsf(wrapf(com.x, w.rx, wl.box.cpu) - cx) - hx, 0.f);
+            float ey = fmaxf(fabsf(wrapf(com.y, w.ry, wl.box.cpu) - cy) - hy, 0.f);
+            float ez = fmaxf(fabsf(wrapf(com.z, w.rz, wl.box.cpu) - cz) - hz, 0.f);
             bool open = lev < 2 || ex * ex + ey * ey + ez * ez < __uint_as_float(com.w);
             if (!open)
               kind = 1;
@@ -785,47 +820,54 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         npcl += cntv;
         __syncwarp();
         if (npcl >= 32) {
-          eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, g12, delta, wmax, npc);
+          eval_pc(wl, npcl, wl.box, w, wl.box.cpi, rs2i, t0, g12, delta, wmax, npc);
           npcl = 0;
         }
       }
-      // particle ranges, one lane at a time
-      unsigned pr = __ballot_sync(0xffffffffu, kind == 3);
-      while (pr) {
-        int src = __ffs(pr) - 1;
-        pr &= pr - 1;
-        uint32_t s = __shfl_sync(0xffffffffu, ps, src);
-        uint32_t c = __shfl_sync(0xffffffffu, pcnt, src);
-        while (c > 0) {
-          uint32_t room = (uint32_t)(kPpBatch - nppl);
-          uint32_t take2 = min(min(room, c), 32u);
-          if ((uint32_t)lane < take2) wl.pp[nppl + lane] = s + lane;
-          nppl += (int)take2;
-          s += take2;
-          c -= take2;
-          __syncwarp();
-          if (nppl == kPpBatch) {
-            eval_pp(wl, nppl, spos, w, cpi, cpu, gbox, rs2i, t0, wmax, npp);
-            nppl = 0;
-          }
+      // particle ranges of all lanes at once: an inclusive scan of the counts
+      // gives each lane its slice of the source list (lane order, as a
+      // one-lane-at-a-time append would), flushed through eval_pp whenever
+      // the batch fills
+      uint32_t cnt = kind == 3 ? pcnt : 0u;
+      uint32_t pincl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, pincl, o);
+        if (lane >= o) pincl += y;
+      }
+      uint32_t ptotal = __shfl_sync(0xffffffffu, pincl, 31);
+      uint32_t pexcl = pincl - cnt;
+      uint32_t done = 0;
+      while (done < ptotal) {
+        uint32_t chunk = min((uint32_t)(kPpBatch - nppl), ptotal - done);
+        uint32_t lo = max(pexcl, done), hi = min(pincl, done + chunk);
+        for (uint32_t g = lo; g < hi; g++) wl.pp[nppl + (int)(g - done)] = ps + (g - pexcl);
+        nppl += (int)chunk;
+        done += chunk;
+        __syncwarp();
+        if (nppl == kPpBatch) {
+          eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpi, wl.box.cpu, gbox, rs2i, t0, wmax, npp);
+          nppl = 0;
         }
       }
     }
     if (failed) {
-      if (lane == 0) atomicOr(err, (uint32_t)kErrStackOverflow);
+      if (lane == 0) atomicOr(wl.box.err, (uint32_t)kErrStackOverflow);
       continue;
     }
-    if (npcl > 0) eval_pc(wl, npcl, tb, w, cpi, rs2i, t0, g12, delta, wmax, npc);
-    if (nppl > 0) eval_pp(wl, nppl, spos, w, cpi, cpu, gbox, rs2i, t0, wmax, npp);
+    if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpi, rs2i, t0, g12, delta, wmax, npc);
+    if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpi, wl.box.cpu, gbox, rs2i, t0, wmax, npp);
     if (w.active) {
-      // the particle sums used separations in index units: back to cells
+      // the particle sums used separations in index units: back to cells;
+      // the table is per unit LL: this box's 1/N^2
       int64_t i = (int64_t)gs + lane;
-      float md = mass * delta;
-      ftree[3 * i + 0] = fmaf(w.ax, md, w.bx);
-      ftree[3 * i + 1] = fmaf(w.ay, md, w.by);
-      ftree[3 * i + 2] = fmaf(w.az, md, w.bz);
+      float md = wl.box.mass * delta, il = wl.box.inv_ll;
+      float *ftree = wl.box.ftree;
+      ftree[3 * i + 0] = fmaf(w.ax, md, w.bx) * il;
+      ftree[3 * i + 1] = fmaf(w.ay, md, w.by) * il;
+      ftree[3 * i + 2] = fmaf(w.az, md, w.bz) * il;
     }
   }
+
   // interaction counters
   for (int o = 16; o > 0; o >>= 1) {
     npp += __shfl_down_sync(0xffffffffu, npp, o);
@@ -834,11 +876,11 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     nvisit += __shfl_down_sync(0xffffffffu, nvisit, o);
   }
   if (lane == 0) {
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[2]), npp);
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[4]), npc);
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[6]), niter / 32);
-    atomicAdd(reinterpret_cast<unsigned long long *>(&tb.counters[8]), nvisit / 32);
-    atomicMax(&tb.counters[10], (uint32_t)max_top);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&stats[2]), npp);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&stats[4]), npc);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&stats[6]), niter / 32);
+    atomicAdd(reinterpret_cast<unsigned long long *>(&stats[8]), nvisit / 32);
+    atomicMax(&stats[10], (uint32_t)max_top);
   }
 }
 
@@ -849,11 +891,12 @@ static int walk_grid(size_t smem) {
   static int cap_set = 0;
   if (!cap_set) {
     size_t max_smem = sizeof(float4) * ((4097 + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
-    cudaFuncSetAttribute(k_tree_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_tree_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_tree_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     cap_set = 1;
   }
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_walk, kWalkThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_walk<true>, kWalkThreads, smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -869,17 +912,72 @@ int64_t walk_stack_words() {
   return (int64_t)sms * 2 * kWalkWarps * (kStackCap - kStackSmem);
 }
 
+WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, const LawTable &law,
+                 float *ftree, uint32_t *err) {
+  WalkBox b;
+  b.spos = spos;
+  b.walkA = tb.walkA;
+  b.walkB = tb.walkB;
+  b.mom0 = tb.mom0;
+  b.mom1 = tb.mom1;
+  b.mom2 = tb.mom2;
+  b.groups = tb.groups;
+  b.ngroups = tb.counters;  // counters[0] = the group count tree_groups wrote
+  b.ftree = ftree;
+  b.err = err;
+  b.cpu = tp.cell_per_unit;
+  b.cpi = tp.cell_per_unit * law.inv_delta;
+  b.mass = tp.mass;
+  b.inv_ll = (float)(1.0 / ((double)tp.n * (double)tp.n));
+  return b;
+}
+
+static void launch_walk(const WalkBox *boxes, const uint32_t *gprefix, int nbox, uint32_t *gnext, uint32_t *stack,
+                        int64_t stack_words, uint32_t *stats, const LawTable &law, float rsphere, cudaStream_t st) {
+  size_t smem = sizeof(float4) * ((law.entries + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
+  int grid = walk_grid(smem);
+  int64_t max_grid = stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
+  if (grid > max_grid) grid = (int)max_grid;
+  if (law.hard_cut)
+    k_tree_walk<true><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
+                                                        law.entries, law.inv_delta, rsphere * rsphere);
+  else
+    k_tree_walk<false><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
+                                                         law.entries, law.inv_delta, rsphere * rsphere);
+}
+
+__global__ void k_set_walkbox(WalkBox *dst, WalkBox v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
+}
+
 void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const TreeBuffers &tb,
                const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st, int64_t *launches) {
   (void)np;
-  size_t smem = sizeof(float4) * ((law.entries + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
-  int grid = walk_grid(smem);
-  int64_t max_grid = tb.stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
-  if (grid > max_grid) grid = (int)max_grid;
-  k_tree_walk<<<grid, kWalkThreads, smem, st>>>(spos, tb, law.t0, law.t12, law.entries, law.inv_delta,
-                                                tp.cell_per_unit, tp.rsphere * tp.rsphere, tp.mass, ftree,
-                                                err);
-  if (launches) *launches += 1;
+  // the box record goes to the device with the launch that precedes the walk
+  k_set_walkbox<<<1, 32, 0, st>>>(tb.walkbox, walk_box(tp, spos, tb, law, ftree, err));
+  // tb.counters[1] is the next-group counter (zeroed before tree_groups)
+  launch_walk(tb.walkbox, nullptr, 1, &tb.counters[1], tb.stack, tb.stack_words, tb.counters, law, tp.rsphere, st);
+  if (launches) *launches += 2;
+}
+
+// Prefix of the boxes' group counts and the launch's next-group counter.
+__global__ void k_group_prefix(const WalkBox *__restrict__ boxes, int nbox, uint32_t *__restrict__ gprefix,
+                               uint32_t *__restrict__ gnext) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    uint32_t run = 0;
+    for (int b = 0; b < nbox; b++) {
+      gprefix[b] = run;
+      run += *boxes[b].ngroups;
+    }
+    gprefix[nbox] = run;
+    *gnext = 0;
+  }
+}
+
+void tree_walk_multi(const WalkBox *boxes, int nbox, uint32_t *gprefix, uint32_t *gnext, uint32_t *stack,
+                     int64_t stack_words, uint32_t *stats, const LawTable &law, float rsphere, cudaStream_t st) {
+  k_group_prefix<<<1, 32, 0, st>>>(boxes, nbox, gprefix, gnext);
+  launch_walk(boxes, gprefix, nbox, gnext, stack, stack_words, stats, law, rsphere, st);
 }
 
 }  // namespace tpm

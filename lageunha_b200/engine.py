@@ -74,6 +74,15 @@ class TpmRequestInfo(ctypes.Structure):
 REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
+class TpmTuning(ctypes.Structure):
+    _fields_ = [("fft_pencils_x", ctypes.c_int32), ("fft_cols", ctypes.c_int32), ("group_level", ctypes.c_int32),
+                ("group_max", ctypes.c_int32), ("ms_fft", ctypes.c_float), ("ms_fft_default", ctypes.c_float),
+                ("ms_walk", ctypes.c_float), ("ms_walk_default", ctypes.c_float)]
+
+
+TUNE_FFT, TUNE_GROUPS = 1, 2
+
+
 class EngineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"tpm error {code}: {msg}")
@@ -121,6 +130,9 @@ _SIGS = {
     "tpm_batch_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.POINTER(ctypes.c_float),
                                       ctypes.POINTER(ctypes.c_float)]),
     "tpm_batch_time": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float)]),
+    "tpm_autotune": (ctypes.c_int, [_P, ctypes.c_uint, ctypes.POINTER(TpmTuning)]),
+    "tpm_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
+    "tpm_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
     "tpm_estimate_bytes": (ctypes.c_int64, [ctypes.c_int32, ctypes.c_int64]),
     "tpm_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "tpm_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(TpmRequest), ctypes.POINTER(ctypes.c_int64)]),
@@ -310,6 +322,21 @@ class Engine:
     def graph_compute(self, parts: int = PART_ALL):
         """tpm_compute_forces replayed from a captured CUDA graph."""
         _check(self._lib.tpm_graph_compute(self._ctx, parts))
+
+    def autotune(self, what: int = TUNE_FFT | TUNE_GROUPS) -> dict:
+        t = TpmTuning()
+        _check(self._lib.tpm_autotune(self._ctx, what, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in TpmTuning._fields_}
+
+    @property
+    def tuning(self) -> TpmTuning:
+        t = TpmTuning()
+        _check(self._lib.tpm_get_tuning(self._ctx, ctypes.byref(t)))
+        return t
+
+    @tuning.setter
+    def tuning(self, t: TpmTuning):
+        _check(self._lib.tpm_set_tuning(self._ctx, ctypes.byref(t)))
 
     def hubble_drag(self, fact1: float):
         _check(self._lib.tpm_hubble_drag(self._ctx, fact1))

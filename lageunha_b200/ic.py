@@ -62,12 +62,40 @@ def from_fixed_point(u: np.ndarray, n: int) -> np.ndarray:
     return u.astype(np.float64) * (float(n) / 4294967296.0)
 
 
+def _displacement_field_torch(white: np.ndarray, spec_index: float, damp: float, rms_target: float,
+                              device: str) -> np.ndarray:
+    """The transforms of _displacement_field done by torch.fft on a GPU
+    (FP64), for the 512^3 workload; same field up to FFT rounding."""
+    import torch
+    n = white.shape[0]
+    wk = torch.fft.rfftn(torch.from_numpy(white).to(device))
+    f = torch.fft.fftfreq(n, dtype=torch.float64, device=device) * 2 * np.pi
+    fr = torch.fft.rfftfreq(n, dtype=torch.float64, device=device) * 2 * np.pi
+    kz, ky, kx = f[:, None, None], f[None, :, None], fr[None, None, :]
+    k2 = kx * kx + ky * ky + kz * kz
+    k2[0, 0, 0] = 1.0
+    amp = torch.pow(k2, spec_index / 4.0) * torch.exp(-0.5 * damp * damp * k2)
+    amp[0, 0, 0] = 0.0
+    dk = wk * amp / k2
+    del wk, amp
+    psi = np.empty((3, n, n, n), dtype=np.float64)
+    for c, kc in enumerate((kx, ky, kz)):
+        psi[c] = torch.fft.irfftn(1j * kc * dk, s=(n, n, n), dim=(0, 1, 2)).cpu().numpy()
+    del dk
+    rms = np.sqrt(np.mean(np.sum(psi * psi, axis=0)))
+    psi *= rms_target / rms
+    return psi
+
+
 def _displacement_field(n: int, rng: np.random.Generator, spec_index: float, damp: float,
-                        rms_target: float) -> np.ndarray:
+                        rms_target: float, device: str | None = None) -> np.ndarray:
     """Zel'dovich displacement psi = IFFT[i k delta_k / k^2] of a Gaussian
     field with P(k) = A k^n exp(-(damp k)^2) (k in radians per cell), scaled so
-    that the rms of |psi| equals rms_target cells. Returns (3, n, n, n) [z][y][x]."""
+    that the rms of |psi| equals rms_target cells. Returns (3, n, n, n) [z][y][x].
+    device: do the transforms with torch on that CUDA device."""
     white = rng.standard_normal((n, n, n), dtype=np.float64)
+    if device is not None:
+        return _displacement_field_torch(white, spec_index, damp, rms_target, device)
     wk = np.fft.rfftn(white)
     kz = 2 * np.pi * np.fft.fftfreq(n)[:, None, None]
     ky = 2 * np.pi * np.fft.fftfreq(n)[None, :, None]
@@ -90,10 +118,11 @@ def _wrap_offset(off: np.ndarray, n: int) -> np.ndarray:
 
 
 def zeldovich(n: int, seed: int, spec_index: float = -2.0, damp: float = 0.5,
-              rms_disp: float = 0.3, box_mpc: float = 100.0, vel_factor: float = 0.0) -> ParticleSet:
+              rms_disp: float = 0.3, box_mpc: float = 100.0, vel_factor: float = 0.0,
+              device: str | None = None) -> ParticleSet:
     """n^3 particles on an n^3 mesh, displaced from the lattice by psi."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    psi = _displacement_field(n, rng, spec_index, damp, rms_disp)
+    psi = _displacement_field(n, rng, spec_index, damp, rms_disp, device)
     # lattice index i + n*(j + n*k) for the point (x=i, y=j, z=k)
     offset = np.stack([psi[0].ravel(), psi[1].ravel(), psi[2].ravel()], axis=1)
     offset = _wrap_offset(offset, n).astype(np.float32)
@@ -183,11 +212,17 @@ def lattice_box(n_lattice: int, n_mesh: int, seed: int, spec_index: float, rms_d
 ENSEMBLE_BOXES = 64
 
 
-def ensemble_box(b: int, max_lattice: int = 160, min_lattice: int = 32) -> Box:
+def ensemble_spec(b: int, max_lattice: int = 160, min_lattice: int = 32) -> tuple:
+    """(lattice size, box size in Mpc/h, spectral index) of ensemble box b."""
     rng = np.random.Generator(np.random.PCG64(4000 + b))
     nl = int(round(np.exp(rng.uniform(np.log(min_lattice), np.log(max_lattice)))))
     box = float(rng.uniform(50.0, 300.0))
     ns = float(rng.uniform(-2.5, -1.5))
+    return nl, box, ns
+
+
+def ensemble_box(b: int, max_lattice: int = 160, min_lattice: int = 32) -> Box:
+    nl, box, ns = ensemble_spec(b, max_lattice, min_lattice)
     return lattice_box(nl, fft_friendly(nl), 4000 + b, ns, 1.0, box, vel_factor=0.5)
 
 
@@ -195,7 +230,7 @@ def ensemble(nbox: int = ENSEMBLE_BOXES, max_lattice: int = 160, min_lattice: in
     return [ensemble_box(b, max_lattice, min_lattice) for b in range(nbox)]
 
 
-def workload(name: str, scale: int | None = None) -> ParticleSet:
+def workload(name: str, scale: int | None = None, device: str | None = None) -> ParticleSet:
     """The named synthetic workloads. `scale` overrides the mesh size (for
     parity-sized cases with the same statistics).
 
@@ -217,5 +252,6 @@ def workload(name: str, scale: int | None = None) -> ParticleSet:
                              nmax=20000 if n >= 128 else 2000)
     if name == "scale512":
         n = scale or 512
-        return zeldovich(n, seed=3, spec_index=-2.5, damp=0.5, rms_disp=2.0, box_mpc=500.0, vel_factor=0.5)
+        return zeldovich(n, seed=3, spec_index=-2.5, damp=0.5, rms_disp=2.0, box_mpc=500.0, vel_factor=0.5,
+                         device=device)
     raise KeyError(name)
