@@ -173,7 +173,26 @@ static int build_law(tpm_ctx *c) {
       hard_cut = 0;
     }
   }
+  // the particle-particle column on the log-spaced r^2 grid, from the same
+  // law (per unit LL), zero from the cut on
+  std::vector<float2> tlog(kLogEntries + 1);
+  {
+    std::vector<double> v(kLogEntries + 1);
+    double rs2 = (double)p.rsphere * (double)p.rsphere;
+    for (int k = 0; k <= kLogEntries; k++) {
+      uint32_t bits = (uint32_t)(kLogBase + k) << kLogShift;
+      float sf;
+      memcpy(&sf, &bits, 4);
+      double s = (double)sf, r = sqrt(s);
+      v[k] = s >= rs2 ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
+    }
+    for (int k = 0; k < kLogEntries; k++)
+      tlog[k] = make_float2((float)v[k], (float)((v[k + 1] - v[k]) * (double)(1 << kLogMantissa)));
+    tlog[kLogEntries] = make_float2(0.f, 0.f);
+  }
   if (c->law.t0 || c->law.t12) CK(cudaStreamSynchronize(c->st));
+  if (c->law.tlog) cudaFree(c->law.tlog);
+  c->law.tlog = nullptr;
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
   c->law.t0 = nullptr;
@@ -182,6 +201,8 @@ static int build_law(tpm_ctx *c) {
   CK(cudaMalloc(&c->law.t12, sizeof(float4) * entries));
   CK(cudaMemcpy(c->law.t0, t0.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->law.t12, t12.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->law.tlog, sizeof(float2) * (kLogEntries + 1)));
+  CK(cudaMemcpy(c->law.tlog, tlog.data(), sizeof(float2) * (kLogEntries + 1), cudaMemcpyHostToDevice));
   c->law.entries = entries;
   c->law.hard_cut = hard_cut;
   c->law.delta = ran2nran;
@@ -573,6 +594,7 @@ int tpm_destroy(tpm_ctx *c) {
   free_mesh(c);
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
+  if (c->law.tlog) cudaFree(c->law.tlog);
   if (c->err) cudaFree(c->err);
   if (c->tb.counters) cudaFree(c->tb.counters);
   if (c->tb.level_range) cudaFree(c->tb.level_range);

@@ -144,9 +144,18 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 // and frac = w - n, column c is diff_c[n] + slope_c[n]*delta*frac
 // (OST/Model4TreeForce.c:34-46). t0 = {diff0, slope0*delta},
 // t12 = {diff1, slope1*delta, diff2, slope2*delta}.
+// The particle-particle column once more, indexed by the float bits of r^2:
+// entry k covers r^2 in [s_k, s_{k+1}) with s_k the float whose top bits are
+// (kLogBase + k) << kLogShift, i.e. 2^kLogMantissa bins per octave of r^2 from
+// 2^-20 to 2^6 cells^2; {value at s_k, (value at s_{k+1} - value) * 2^kLogMantissa}.
+constexpr int kLogMantissa = 7;
+constexpr int kLogShift = 23 - kLogMantissa;
+constexpr int kLogBase = (127 - 20) << kLogMantissa;
+constexpr int kLogEntries = 26 << kLogMantissa;
 struct LawTable {
   float2 *t0 = nullptr;
   float4 *t12 = nullptr;
+  float2 *tlog = nullptr;  // [kLogEntries + 1]
   int entries = 0;
   float delta = 0, inv_delta = 0;
   // 1: the walk tests r <= rsphere per pair (the reference's cut);

@@ -461,6 +461,7 @@ constexpr int kStackSmem = 640;    // per-warp stack entries in shared memory
 constexpr int kStackCap = 8192;    // entries beyond kStackSmem live in global memory
 constexpr int kPcCap = 64;
 constexpr int kPpBatch = 96;       // particle sources evaluated per flush
+constexpr int kLogSmemF4 = (kLogEntries + 2) / 2;  // the log-spaced table, in float4s
 
 struct WarpLists {
   WalkBox box;                     // the box of the group this warp walks
@@ -471,9 +472,9 @@ struct WarpLists {
 };
 
 struct WalkCtx {
-  float tx, ty, tz;       // this lane's target relative to u_ref (table-index units)
-  float ax, ay, az;       // particle-particle sum (index units, without the particle mass)
-  float bx, by, bz;       // particle-node sum (cells)
+  float tx, ty, tz;       // this lane's target relative to u_ref (cells)
+  float ax, ay, az;       // particle-particle sum (without the particle mass)
+  float bx, by, bz;       // particle-node sum
   bool active;
   uint32_t rx, ry, rz;    // u_ref
 };
@@ -486,8 +487,9 @@ TPM_D float rsqrt_approx(float x) {
   return y;
 }
 
-// Table lookup at w = r/delta (w >= 0) without float<->int conversions:
-// adding 1.5*2^23 rounding toward -inf leaves floor(w) in the low mantissa.
+// Linear-table lookup at w = r/delta (w >= 0) without float<->int
+// conversions: adding 1.5*2^23 rounding toward -inf leaves floor(w) in the
+// low mantissa.
 TPM_D int table_index(float w, float &frac) {
   const float magic = 12582912.0f;
   float v = __fadd_rd(w, magic);
@@ -497,21 +499,22 @@ TPM_D int table_index(float w, float &frac) {
 }
 
 // One source against this lane's target: the reference's AddPar
-// (OST/ost.ver2.c:279-293) without the mass factor, masked to r^2 <= rs^2.
-// Coordinates are in table-index units (cells / delta); r2 = 0 (the target
-// itself) gives rsqrt = inf, w = NaN, which fminf turns into wmax, and a zero
-// separation, so it adds nothing.
-// kHardCut: the per-pair r^2 <= rsphere^2 test of the reference law; a table
-// that already falls to zero at the cut (the Gaussian law's) needs none.
+// (OST/ost.ver2.c:279-293) without the mass factor. The law comes from the
+// table indexed by the float bits of r^2 (cells^2): the exponent and the top
+// kLogMantissa mantissa bits pick the bin, the remaining mantissa bits are the
+// position inside it, so neither a square root nor a conversion is needed.
+// r2 = 0 (the target itself) lands in bin 0 with a zero separation, adding
+// nothing. kHardCut: the per-pair r^2 <= rsphere^2 test of the reference law;
+// the table is zero from the cut on, which is all the Gaussian law needs.
 template <bool kHardCut>
-TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, float wmax, const float2 *__restrict__ t0,
-                   float &ax, float &ay, float &az) {
+TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, const float2 *__restrict__ tl, float &ax,
+                   float &ay, float &az) {
   float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  float wq = fminf(r2 * rsqrt_approx(r2), wmax);
-  float frac;
-  int nt = table_index(wq, frac);
-  float2 c = t0[nt];
+  uint32_t bits = __float_as_uint(r2);
+  int k = min(max((int)(bits >> kLogShift) - kLogBase, 0), kLogEntries);
+  float frac = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u) - 1.f;
+  float2 c = tl[k];
   float f = fmaf(c.y, frac, c.x);
   if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
@@ -532,9 +535,8 @@ struct GroupBox {
 // lane), and the kept ones are compacted, in order, into wl.stage; then every
 // lane evaluates every kept source against its target.
 template <bool kHardCut>
-TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpi, float cpu,
-                   const GroupBox &gb, float rs2, const float2 *__restrict__ t0, float wmax,
-                   unsigned long long &npp) {
+TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
+                   const GroupBox &gb, float rs2, const float2 *__restrict__ tl, unsigned long long &npp) {
   int lane = threadIdx.x & 31;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
   // all loads of the batch are issued before any is used
@@ -554,16 +556,18 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
   for (int b = 0; b < kPpBatch / 32; b++) {
     int k = b * 32 + lane;
     bool keep = false;
+    float px = 0.f, py = 0.f, pz = 0.f;
     if (k < m) {
-      float dx = fmaxf(fabsf(wrapf(u[b][0], w.rx, cpu) - gb.cx) - gb.hx, 0.f);
-      float dy = fmaxf(fabsf(wrapf(u[b][1], w.ry, cpu) - gb.cy) - gb.hy, 0.f);
-      float dz = fmaxf(fabsf(wrapf(u[b][2], w.rz, cpu) - gb.cz) - gb.hz, 0.f);
+      px = wrapf(u[b][0], w.rx, cpu);
+      py = wrapf(u[b][1], w.ry, cpu);
+      pz = wrapf(u[b][2], w.rz, cpu);
+      float dx = fmaxf(fabsf(px - gb.cx) - gb.hx, 0.f);
+      float dy = fmaxf(fabsf(py - gb.cy) - gb.hy, 0.f);
+      float dz = fmaxf(fabsf(pz - gb.cz) - gb.hz, 0.f);
       keep = dx * dx + dy * dy + dz * dz <= gb.reach2;
     }
     unsigned mk = __ballot_sync(0xffffffffu, keep);
-    if (keep)
-      wl.stage[kept + __popc(mk & lanemask_lt)] =
-          make_float4(wrapf(u[b][0], w.rx, cpi), wrapf(u[b][1], w.ry, cpi), wrapf(u[b][2], w.rz, cpi), 0.f);
+    if (keep) wl.stage[kept + __popc(mk & lanemask_lt)] = make_float4(px, py, pz, 0.f);
     kept += __popc(mk);
   }
   __syncwarp();
@@ -572,12 +576,12 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
   float a2x = 0.f, a2y = 0.f, a2z = 0.f, a3x = 0.f, a3y = 0.f, a3z = 0.f;
   int j = 0;
   for (; j + 4 <= m; j += 4) {
-    pp_body<kHardCut>(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
-    pp_body<kHardCut>(wl.stage[j + 1], w, rs2, wmax, t0, a1x, a1y, a1z);
-    pp_body<kHardCut>(wl.stage[j + 2], w, rs2, wmax, t0, a2x, a2y, a2z);
-    pp_body<kHardCut>(wl.stage[j + 3], w, rs2, wmax, t0, a3x, a3y, a3z);
+    pp_body<kHardCut>(wl.stage[j], w, rs2, tl, a0x, a0y, a0z);
+    pp_body<kHardCut>(wl.stage[j + 1], w, rs2, tl, a1x, a1y, a1z);
+    pp_body<kHardCut>(wl.stage[j + 2], w, rs2, tl, a2x, a2y, a2z);
+    pp_body<kHardCut>(wl.stage[j + 3], w, rs2, tl, a3x, a3y, a3z);
   }
-  for (; j < m; j++) pp_body<kHardCut>(wl.stage[j], w, rs2, wmax, t0, a0x, a0y, a0z);
+  for (; j < m; j++) pp_body<kHardCut>(wl.stage[j], w, rs2, tl, a0x, a0y, a0z);
   if (w.active) {
     w.ax += (a0x + a1x) + (a2x + a3x);
     w.ay += (a0y + a1y) + (a2y + a3y);
@@ -588,10 +592,10 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 }
 
 // Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
-// and z components on their own axes. Coordinates are in table-index units;
-// the separations are rescaled to cells with delta for the force terms.
-TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpi, float rs2,
-                   const float2 *__restrict__ t0, const float4 *__restrict__ t12, float delta,
+// and z components on their own axes. Coordinates are in cells; the linear
+// tables (t0, t12, index w = r / delta) give the law and its derivatives.
+TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpu, float rs2,
+                   const float2 *__restrict__ t0, const float4 *__restrict__ t12, float inv_delta,
                    float wmax, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
   for (int base = 0; base < m_all; base += 32) {
@@ -599,9 +603,9 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, floa
     if (lane < m) {
       uint32_t nd = wl.pc[base + lane];
       float4 m0 = tb.mom0[nd], m1 = tb.mom1[nd], m2 = tb.mom2[nd];
-      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpi),
-                                           wrapf(__float_as_uint(m0.y), w.ry, cpi),
-                                           wrapf(__float_as_uint(m0.z), w.rz, cpi), m0.w);
+      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpu),
+                                           wrapf(__float_as_uint(m0.y), w.ry, cpu),
+                                           wrapf(__float_as_uint(m0.z), w.rz, cpu), m0.w);
       wl.stage[3 * lane + 1] = m1;  // Qxx Qyy Qzz Qxy
       wl.stage[3 * lane + 2] = m2;  // Qxz Qyz trQ mass
     }
@@ -609,13 +613,12 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, floa
     float ax = 0.f, ay = 0.f, az = 0.f;
     for (int j = 0; j < m; j++) {
       float4 c0 = wl.stage[3 * j], q1 = wl.stage[3 * j + 1], q2 = wl.stage[3 * j + 2];
-      float ux = w.tx - c0.x, uy = w.ty - c0.y, uz = w.tz - c0.z;
-      float r2 = fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-      float wq = fminf(r2 * rsqrt_approx(r2), wmax);
-      float dx = ux * delta, dy = uy * delta, dz = uz * delta;
+      float dx = w.tx - c0.x, dy = w.ty - c0.y, dz = w.tz - c0.z;
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float wq = fminf(r2 * rsqrt_approx(r2) * inv_delta, wmax);
       float frac;
       int nt = table_index(wq, frac);
-      float2 c = t0[nt];
+      float2 c = __ldg(&t0[nt]);
       float4 d = __ldg(&t12[nt]);
       float f1 = fmaf(c.y, frac, c.x), f2 = fmaf(d.y, frac, d.x), f3 = fmaf(d.w, frac, d.z);
       float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
@@ -662,13 +665,12 @@ template <bool kHardCut>
 __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     const WalkBox *__restrict__ boxes, const uint32_t *__restrict__ gprefix, int nbox,
     uint32_t *__restrict__ gnext, uint32_t *__restrict__ stack_base, uint32_t *__restrict__ stats,
-    const float2 *__restrict__ g0, const float4 *__restrict__ g12, int entries, float inv_delta, float rs2) {
-  const float rs2i = rs2 * inv_delta * inv_delta;
-  const float delta = 1.f / inv_delta;
+    const float2 *__restrict__ g0, const float4 *__restrict__ g12, const float2 *__restrict__ glog, int entries,
+    float inv_delta, float rs2) {
   extern __shared__ float4 smem4[];
-  float2 *t0 = reinterpret_cast<float2 *>(smem4);
-  WarpLists *lists = reinterpret_cast<WarpLists *>(smem4 + (entries + 2) / 2);
-  for (int i = threadIdx.x; i <= entries; i += kWalkThreads) t0[i] = g0[i];
+  float2 *tl = reinterpret_cast<float2 *>(smem4);
+  WarpLists *lists = reinterpret_cast<WarpLists *>(smem4 + kLogSmemF4);
+  for (int i = threadIdx.x; i <= kLogEntries; i += kWalkThreads) tl[i] = glog[i];
   __syncthreads();
   const float wmax = (float)(entries - 1);
   int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -721,16 +723,13 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     w.rx = __shfl_sync(0xffffffffu, ux, 0);
     w.ry = __shfl_sync(0xffffffffu, uy, 0);
     w.rz = __shfl_sync(0xffffffffu, uz, 0);
-    w.tx = w.active ? wrapf(ux, w.rx, wl.box.cpi) : 0.f;
-    w.ty = w.active ? wrapf(uy, w.ry, wl.box.cpi) : 0.f;
-    w.tz = w.active ? wrapf(uz, w.rz, wl.box.cpi) : 0.f;
+    w.tx = w.active ? wrapf(ux, w.rx, wl.box.cpu) : 0.f;
+    w.ty = w.active ? wrapf(uy, w.ry, wl.box.cpu) : 0.f;
+    w.tz = w.active ? wrapf(uz, w.rz, wl.box.cpu) : 0.f;
     w.ax = w.ay = w.az = 0.f;
     w.bx = w.by = w.bz = 0.f;
     // group box in cells
-    float gx0 = w.active ? wrapf(ux, w.rx, wl.box.cpu) : 0.f;
-    float gy0 = w.active ? wrapf(uy, w.ry, wl.box.cpu) : 0.f;
-    float gz0 = w.active ? wrapf(uz, w.rz, wl.box.cpu) : 0.f;
-    float lox = gx0, hix = gx0, loy = gy0, hiy = gy0, loz = gz0, hiz = gz0;
+    float lox = w.tx, hix = w.tx, loy = w.ty, hiy = w.ty, loz = w.tz, hiz = w.tz;
     for (int o = 16; o > 0; o >>= 1) {
       lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
       hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
@@ -820,7 +819,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         npcl += cntv;
         __syncwarp();
         if (npcl >= 32) {
-          eval_pc(wl, npcl, wl.box, w, wl.box.cpi, rs2i, t0, g12, delta, wmax, npc);
+          eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, g0, g12, inv_delta, wmax, npc);
           npcl = 0;
         }
       }
@@ -845,7 +844,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         done += chunk;
         __syncwarp();
         if (nppl == kPpBatch) {
-          eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpi, wl.box.cpu, gbox, rs2i, t0, wmax, npp);
+          eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, tl, npp);
           nppl = 0;
         }
       }
@@ -854,13 +853,12 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
       if (lane == 0) atomicOr(wl.box.err, (uint32_t)kErrStackOverflow);
       continue;
     }
-    if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpi, rs2i, t0, g12, delta, wmax, npc);
-    if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpi, wl.box.cpu, gbox, rs2i, t0, wmax, npp);
+    if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, g0, g12, inv_delta, wmax, npc);
+    if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, tl, npp);
     if (w.active) {
-      // the particle sums used separations in index units: back to cells;
-      // the table is per unit LL: this box's 1/N^2
+      // the tables are per unit LL: this box's 1/N^2
       int64_t i = (int64_t)gs + lane;
-      float md = wl.box.mass * delta, il = wl.box.inv_ll;
+      float md = wl.box.mass, il = wl.box.inv_ll;
       float *ftree = wl.box.ftree;
       ftree[3 * i + 0] = fmaf(w.ax, md, w.bx) * il;
       ftree[3 * i + 1] = fmaf(w.ay, md, w.by) * il;
@@ -890,7 +888,7 @@ static int walk_grid(size_t smem) {
   // different tables stay launchable whatever order they were made in.
   static int cap_set = 0;
   if (!cap_set) {
-    size_t max_smem = sizeof(float4) * ((4097 + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
+    size_t max_smem = sizeof(float4) * kLogSmemF4 + sizeof(WarpLists) * kWalkWarps;
     cudaFuncSetAttribute(k_tree_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     cudaFuncSetAttribute(k_tree_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     cap_set = 1;
@@ -934,16 +932,16 @@ WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &
 
 static void launch_walk(const WalkBox *boxes, const uint32_t *gprefix, int nbox, uint32_t *gnext, uint32_t *stack,
                         int64_t stack_words, uint32_t *stats, const LawTable &law, float rsphere, cudaStream_t st) {
-  size_t smem = sizeof(float4) * ((law.entries + 2) / 2) + sizeof(WarpLists) * kWalkWarps;
+  size_t smem = sizeof(float4) * kLogSmemF4 + sizeof(WarpLists) * kWalkWarps;
   int grid = walk_grid(smem);
   int64_t max_grid = stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
   if (grid > max_grid) grid = (int)max_grid;
   if (law.hard_cut)
     k_tree_walk<true><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
-                                                        law.entries, law.inv_delta, rsphere * rsphere);
+                                                        law.tlog, law.entries, law.inv_delta, rsphere * rsphere);
   else
     k_tree_walk<false><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
-                                                         law.entries, law.inv_delta, rsphere * rsphere);
+                                                         law.tlog, law.entries, law.inv_delta, rsphere * rsphere);
 }
 
 __global__ void k_set_walkbox(WalkBox *dst, WalkBox v) {
