@@ -247,7 +247,8 @@ def run_batched(args, E, ic, law, local):
         tbd.append(batch.last_ms * 1e-3)
     ms_step = None
     cosmo = E.cosmology()
-    batch.step(cosmo, 5.0, 0.02)
+    steps = [0.05 / (float(np.sqrt(np.mean(np.square(b.vel, dtype=np.float64)))) * b.n_mesh) for b in boxes]
+    batch.step(cosmo, 5.0, steps)
     ms_step = batch.last_ms
     # accuracy: FP64 Ewald on 1024 targets of a small, a middle and the largest box
     order = sorted(range(len(boxes)), key=lambda i: boxes[i].np)
@@ -318,9 +319,11 @@ def run_served(args, E, ic, law, local):
         delay = arrivals[r] - (time.perf_counter() - start)
         if delay > 0:
             time.sleep(delay)
+        # steps sized for a 0.05-cell rms drift, as the KDK block does
+        vrms = float(np.sqrt(np.mean(np.square(box.vel, dtype=np.float64))))
         ids.append(srv.submit(pos.numpy().view(np.uint32), vel.numpy(), n_mesh=box.n_mesh, nsteps=nsteps, anow=4.0,
-                              astep=0.02, cosmo=cosmo, pos_out=po.numpy().view(np.uint32), vel_out=vo.numpy(),
-                              epsilon=EPS, **law))
+                              astep=0.05 / (vrms * box.n_mesh), cosmo=cosmo, pos_out=po.numpy().view(np.uint32),
+                              vel_out=vo.numpy(), epsilon=EPS, **law))
     srv.wait(-1, 3600.0)
     infos = [srv.info(i) for i in ids]
     stats = srv.stats()
@@ -527,22 +530,25 @@ def run_engine_arm(args):
                    "reasons": clocks.get("reasons", [])},
     }
     # ---- KDK global steps of the same box (drag, forces, kicks, drift),
-    # velocities of the workload, anow from 5 in steps of 0.02
+    # velocities of the workload, anow from 5; the step is sized so that the
+    # first drift moves particles by 0.05 cells rms (0.02 for a cold start)
     cosmo = E.cosmology()
     eng.set_params(**law)
     vel_dev = torch.from_numpy(ps.vel).to(f"cuda:{local}")
     eng.load_fixed(pos_dev, vel_dev)
-    eng.step(cosmo, 5.0, 0.02, 0)
+    vrms = float(np.sqrt(np.mean(np.square(ps.vel, dtype=np.float64))))
+    astep = 0.05 / (vrms * n) if vrms > 0 else 0.02
+    eng.step(cosmo, 5.0, astep, 0)
     nk = max(1, args.kdk_steps)
     barrier()
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
     k0.record(stream)
     for s in range(nk):
-        eng.step(cosmo, 5.02 + 0.02 * s, 0.02, 1 + s)
+        eng.step(cosmo, 5.0 + astep * (1 + s), astep, 1 + s)
     k1.record(stream)
     barrier()
-    line["kdk"] = {"steps": nk, "ms_per_step": k0.elapsed_time(k1) / nk,
+    line["kdk"] = {"steps": nk, "astep": astep, "anow": 5.0, "ms_per_step": k0.elapsed_time(k1) / nk,
                    "value": ws * npart * nk / (k0.elapsed_time(k1) * 1e-3) / 1e6, "unit": UNIT}
     if err is not None and nk >= 1:
         # accuracy after the steps, on the moved particles
