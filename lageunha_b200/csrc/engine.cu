@@ -723,13 +723,9 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     launch_range_table(c->skey, np, 3 * (g.sub_bits + 3), ntiles, c->tile_start, st);
     CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
     const bool il = c->prm.law == TPM_LAW_GAUSSIAN;  // interlaced pair of grids
-    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st, 0);
+    if (il) CK(cudaMemsetAsync(c->rho2, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
+    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st, il ? c->rho2 : nullptr);
     c->launches += 2;
-    if (il) {
-      CK(cudaMemsetAsync(c->rho2, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
-      launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho2, st, 1);
-      c->launches += 1;
-    }
     CK(stage_check(st, "deposit"));
     if (timing) CK(cudaEventRecord(c->ev[2], st));
     if (il)

@@ -56,10 +56,10 @@ constexpr int kGhost = 8;    // ghost layers of the padded potential (8-point st
 
 MeshGeom make_geom(int n);
 
-// half != 0 deposits the particles moved by half a cell along every axis (the
-// second grid of the interlaced pair).
+// With rho2 the particles also go onto the second grid of the interlaced pair,
+// moved by half a cell along every axis (a second launch).
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
-                        float mass, float *rho, cudaStream_t st, int half);
+                        float mass, float *rho, cudaStream_t st, float *rho2 = nullptr);
 // FFT pipeline: rho (n^3 real) -> phi_pad (ghosted potential).
 struct FftPlan {
   float2 *tw = nullptr;   // twiddles exp(-2 pi i k / L) for L = n and L = n/2

@@ -79,105 +79,75 @@ constexpr int kDepNy = kTile + 3;     // y/z extent: [t-1, t+9]
 constexpr int kDepCells = kDepNx * kDepNy * kDepNy;
 constexpr int kDepThreads = 256;
 
-__global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
-    const uint32_t *__restrict__ spos, const uint32_t *__restrict__ tile_start, int n, int cbits,
-    float mass, float *__restrict__ rho, int vec4, uint32_t half) {
-  __shared__ float acc[kDepCells];
-  int tid = threadIdx.x, lane = tid & 31;
-  // Morton tile index -> tile coordinates
-  uint32_t t = blockIdx.x;
-  uint32_t tx = 0, ty = 0, tz = 0;
-  for (int b = 0; b < cbits - 3; b++) {
-    tx |= ((t >> (3 * b)) & 1u) << b;
-    ty |= ((t >> (3 * b + 1)) & 1u) << b;
-    tz |= ((t >> (3 * b + 2)) & 1u) << b;
-  }
-  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
-  if (p0 == p1) return;
-  int ox = (int)tx * kTile - 4, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
-  for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0.f;
-  __syncthreads();
-  uint32_t nu = (uint32_t)n;
-  int nwarp_items = (int)((p1 - p0 + 31) / 32) * 32;
-  for (int base = 0; base < nwarp_items; base += kDepThreads) {
-    int k = base + tid;
-    bool valid = (uint32_t)k < p1 - p0;
-    // per-axis weights on offsets -1, 0, +1 around the home node
-    float wx[3] = {0, 0, 0}, wy[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
-    int hx = 0, hy = 0, hz = 0;
+// Per-axis weights on offsets -1, 0, +1 around the home node of a particle,
+// with or without the half-cell shift of the second interlaced grid.
+TPM_D void tsc_axis3(uint32_t u, uint32_t n, uint32_t half, float scale, float w[3], int &near) {
+  Axis a = axis_of(u, n, half);
+  float w1, w2, w3;
+  int s;
+  tsc_w(a.xmin, w1, w2, w3, s);
+  w[1] = w1 * scale;
+  w[1 + s] = w2 * scale;
+  w[1 - s] = w3 * scale;
+  near = a.near;
+}
+
+// Adds the 27 weights of every valid lane to acc, merging runs of lanes with
+// the same home node by a warp segmented sum first (dense clumps put many
+// particles on one node).
+TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], const float wy[3],
+                         const float wz[3], int lane) {
+  int key = valid ? home : -1 - lane;
+  int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  bool head = lane == 0 || prev != key;
+  unsigned heads = __ballot_sync(0xffffffffu, head);
+  if (heads == 0xffffffffu) {
     if (valid) {
-      int64_t i = (int64_t)p0 + k;
-      Axis ax = axis_of(spos[3 * i + 0], nu, half), ay = axis_of(spos[3 * i + 1], nu, half),
-           az = axis_of(spos[3 * i + 2], nu, half);
-      float w1, w2, w3;
-      int s;
-      tsc_w(ax.xmin, w1, w2, w3, s);
-      wx[1] = w1 * mass;
-      wx[1 + s] = w2 * mass;
-      wx[1 - s] = w3 * mass;
-      tsc_w(ay.xmin, w1, w2, w3, s);
-      wy[1] = w1;
-      wy[1 + s] = w2;
-      wy[1 - s] = w3;
-      tsc_w(az.xmin, w1, w2, w3, s);
-      wz[1] = w1;
-      wz[1 + s] = w2;
-      wz[1 - s] = w3;
-      hx = ax.near - ox;
-      hy = ay.near - oy;
-      hz = az.near - oz;
-    }
-    int home = valid ? hx + kDepNx * (hy + kDepNy * hz) : -1 - lane;
-    int prev = __shfl_up_sync(0xffffffffu, home, 1);
-    bool head = lane == 0 || prev != home;
-    unsigned heads = __ballot_sync(0xffffffffu, head);
-    if (heads == 0xffffffffu) {
-      if (valid) {
-        for (int c = 0; c < 3; c++)
-          for (int b = 0; b < 3; b++)
-            for (int a = 0; a < 3; a++)
-              atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))],
-                        wx[a] * wy[b] * wz[c]);
-      }
-    } else {
-      // runs of equal home node: segmented sum onto the run's first lane
-      unsigned le = heads & ((2u << lane) - 1u);
-      int seg = 31 - __clz(le);
-      bool ok[5];
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        int o = 1 << j;
-        int s2 = __shfl_down_sync(0xffffffffu, seg, o);
-        ok[j] = (lane + o < 32) && s2 == seg;
-      }
-      float w[27];
-#pragma unroll
       for (int c = 0; c < 3; c++)
-#pragma unroll
         for (int b = 0; b < 3; b++)
+          for (int a = 0; a < 3; a++)
+            atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], wx[a] * wy[b] * wz[c]);
+    }
+    return;
+  }
+  // runs of equal home node: segmented sum onto the run's first lane
+  unsigned le = heads & ((2u << lane) - 1u);
+  int seg = 31 - __clz(le);
+  bool ok[5];
 #pragma unroll
-          for (int a = 0; a < 3; a++) w[a + 3 * b + 9 * c] = wx[a] * wy[b] * wz[c];
+  for (int j = 0; j < 5; j++) {
+    int o = 1 << j;
+    int s2 = __shfl_down_sync(0xffffffffu, seg, o);
+    ok[j] = (lane + o < 32) && s2 == seg;
+  }
+  float w[27];
 #pragma unroll
-      for (int j = 0; j < 5; j++) {
+  for (int c = 0; c < 3; c++)
 #pragma unroll
-        for (int q = 0; q < 27; q++) {
-          float y = __shfl_down_sync(0xffffffffu, w[q], 1 << j);
-          if (ok[j]) w[q] += y;
-        }
-      }
-      if (valid && head) {
+    for (int b = 0; b < 3; b++)
 #pragma unroll
-        for (int c = 0; c < 3; c++)
+      for (int a = 0; a < 3; a++) w[a + 3 * b + 9 * c] = wx[a] * wy[b] * wz[c];
 #pragma unroll
-          for (int b = 0; b < 3; b++)
+  for (int j = 0; j < 5; j++) {
 #pragma unroll
-            for (int a = 0; a < 3; a++)
-              atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], w[a + 3 * b + 9 * c]);
-      }
+    for (int q = 0; q < 27; q++) {
+      float y = __shfl_down_sync(0xffffffffu, w[q], 1 << j);
+      if (ok[j]) w[q] += y;
     }
   }
-  __syncthreads();
-  // flush to the periodic mesh
+  if (valid && head) {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int b = 0; b < 3; b++)
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+          atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], w[a + 3 * b + 9 * c]);
+  }
+}
+
+// Adds a tile's shared-memory accumulator to the periodic mesh.
+TPM_D void flush_tile(const float *acc, float *__restrict__ rho, int n, int ox, int oy, int oz, int vec4, int tid) {
   if (vec4) {
     for (int i = tid; i < kDepCells / 4; i += kDepThreads) {
       int xq = i % (kDepNx / 4), r = i / (kDepNx / 4);
@@ -203,12 +173,60 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
   }
 }
 
+// TSC deposit of one 8^3 Morton tile; half != 0: the particles moved by half
+// a cell (the second grid of the interlaced pair). One grid per launch: a
+// kernel holding both grids' accumulators ran slower (fewer blocks per SM).
+__global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
+    const uint32_t *__restrict__ spos, const uint32_t *__restrict__ tile_start, int n, int cbits,
+    float mass, float *__restrict__ rho, uint32_t half, int vec4) {
+  __shared__ __align__(16) float acc[kDepCells];
+  int tid = threadIdx.x, lane = tid & 31;
+  // Morton tile index -> tile coordinates
+  uint32_t t = blockIdx.x;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  for (int b = 0; b < cbits - 3; b++) {
+    tx |= ((t >> (3 * b)) & 1u) << b;
+    ty |= ((t >> (3 * b + 1)) & 1u) << b;
+    tz |= ((t >> (3 * b + 2)) & 1u) << b;
+  }
+  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
+  if (p0 == p1) return;
+  int ox = (int)tx * kTile - 4, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
+  for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0.f;
+  __syncthreads();
+  uint32_t nu = (uint32_t)n;
+  int nwarp_items = (int)((p1 - p0 + 31) / 32) * 32;
+  for (int base = 0; base < nwarp_items; base += kDepThreads) {
+    int k = base + tid;
+    bool valid = (uint32_t)k < p1 - p0;
+    uint32_t u[3] = {0u, 0u, 0u};
+    if (valid) {
+      int64_t i = (int64_t)p0 + k;
+      u[0] = spos[3 * i + 0];
+      u[1] = spos[3 * i + 1];
+      u[2] = spos[3 * i + 2];
+    }
+    float wx[3] = {0, 0, 0}, wy[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+    int home = 0;
+    if (valid) {
+      int hx, hy, hz;
+      tsc_axis3(u[0], nu, half, mass, wx, hx);
+      tsc_axis3(u[1], nu, half, 1.f, wy, hy);
+      tsc_axis3(u[2], nu, half, 1.f, wz, hz);
+      home = (hx - ox) + kDepNx * ((hy - oy) + kDepNy * (hz - oz));
+    }
+    deposit_lanes(acc, valid, home, wx, wy, wz, lane);
+  }
+  __syncthreads();
+  flush_tile(acc, rho, n, ox, oy, oz, vec4, tid);
+}
+
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
-                        float mass, float *rho, cudaStream_t st, int half) {
+                        float mass, float *rho, cudaStream_t st, float *rho2) {
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
   int vec4 = (g.n % 4) == 0;
-  k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho, vec4,
-                                                (uint32_t)half);
+  k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho, 0u, vec4);
+  if (rho2) k_tsc_deposit<<<ntiles, kDepThreads, 0, st>>>(spos, tile_start, g.n, g.cbits, mass, rho2, 1u, vec4);
 }
 
 // ------------------------------------------------------------------ FFT

@@ -101,70 +101,108 @@ __global__ void __launch_bounds__(1024) k_radix_scan_digit(uint32_t *__restrict_
   if (tid == 0) dtotal[blockIdx.x] = carry;
 }
 
-// Stable scatter. The tile is consumed in kSortItems rounds of 256 items in
-// index order; inside a round an item's rank among equal digits is
-// (items of that digit in earlier rounds) + (in earlier warps) + (in lower
-// lanes of its warp), so the relative order of equal digits is kept.
+// Stable scatter of one tile of kSortTile items. Warp w owns the contiguous
+// items [w*512, (w+1)*512) of the tile and ranks them in chunks of 32 against
+// its own running digit counts (no block barrier per chunk); a prefix over the
+// warps and over the digits then gives every item its place in the tile
+// sorted by digit, which is written to shared memory. The tile is finally
+// written out in that order, so each digit's run goes to consecutive global
+// addresses. Items of equal digit keep their input order (chunks in order,
+// lanes in order, warps in order), so the pass is a stable sort.
+constexpr int kScatterWarps = kSortThreads / 32;
+constexpr int kWarpItems = kSortTile / kScatterWarps;
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
     const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin, uint64_t *__restrict__ kout,
     uint32_t *__restrict__ vout, int64_t np, int shift, const uint32_t *__restrict__ hist,
     const uint32_t *__restrict__ dtotal, int64_t ntiles) {
-  __shared__ uint32_t base[256];   // global offset of each digit for this tile
-  __shared__ uint32_t wcnt[8][256];
+  extern __shared__ __align__(16) unsigned char sc_smem[];
+  uint64_t *sk = reinterpret_cast<uint64_t *>(sc_smem);                 // [kSortTile] keys in digit order
+  uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kSortTile);          // [kSortTile] values
+  uint16_t *rk = reinterpret_cast<uint16_t *>(sv + kSortTile);          // [kSortTile] rank in warp's digit
+  uint32_t(*wc)[256] = reinterpret_cast<uint32_t(*)[256]>(rk + kSortTile);  // [warps][256]
+  __shared__ uint32_t lstart[256];  // first slot of each digit in the tile
+  __shared__ uint32_t gbase[256];   // global slot of each digit's first item of this tile
+  __shared__ uint32_t ws[kScatterWarps];
   int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < kScatterWarps * 256; i += kSortThreads) (&wc[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t tbase = blockIdx.x * (int64_t)kSortTile;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+  // ---- ranks inside each warp's segment
+  for (int c = 0; c < kWarpItems / 32; c++) {
+    int j = warp * kWarpItems + c * 32 + lane;
+    int64_t i = tbase + j;
+    bool valid = i < np;
+    uint32_t d = valid ? (uint32_t)(kin[i] >> shift) & 0xffu : 0x100u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t prev = valid ? wc[warp][d] : 0u;
+    __syncwarp();
+    if (valid && (peers & lanemask_lt) == 0) wc[warp][d] = prev + __popc(peers);
+    __syncwarp();
+    rk[j] = (uint16_t)(prev + __popc(peers & lanemask_lt));
+  }
+  __syncthreads();
+  // ---- per digit: prefix over the warps, the tile's count, and its global base
+  uint32_t cnt;
   {
-    // digit start = exclusive scan of dtotal (256 entries) + this tile's offset
-    uint32_t v = dtotal[tid];
-    uint32_t x = v;
+    int d = tid;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kScatterWarps; w++) {
+      uint32_t t = wc[w][d];
+      wc[w][d] = run;
+      run += t;
+    }
+    cnt = run;
+    // exclusive scans over the 256 digits: tile counts and global digit totals
+    uint32_t x = cnt, g = dtotal[d];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      uint32_t h = __shfl_up_sync(0xffffffffu, g, o);
+      if (lane >= o) {
+        x += y;
+        g += h;
+      }
     }
-    __shared__ uint32_t ws[8];
     if (lane == 31) ws[warp] = x;
+    __shared__ uint32_t wg[kScatterWarps];
+    if (lane == 31) wg[warp] = g;
     __syncthreads();
-    uint32_t pre = 0;
-    for (int w = 0; w < warp; w++) pre += ws[w];
-    base[tid] = pre + x - v + hist[(int64_t)tid * ntiles + blockIdx.x];
+    uint32_t px = 0, pg = 0;
+    for (int w = 0; w < warp; w++) {
+      px += ws[w];
+      pg += wg[w];
+    }
+    lstart[d] = px + x - cnt;
+    gbase[d] = pg + g - dtotal[d] + hist[(int64_t)d * ntiles + blockIdx.x];
   }
   __syncthreads();
-  int64_t tbase = blockIdx.x * (int64_t)kSortTile;
-  uint32_t lanemask_lt = (1u << lane) - 1u;
-  for (int r = 0; r < kSortItems; r++) {
-    for (int i = tid; i < 8 * 256; i += kSortThreads) (&wcnt[0][0])[i] = 0;
-    __syncthreads();
-    int64_t i = tbase + r * kSortThreads + tid;
-    bool valid = i < np;
-    uint64_t k = valid ? kin[i] : 0ull;
-    uint32_t v = valid ? vin[i] : 0u;
-    uint32_t d = valid ? (uint32_t)(k >> shift) & 0xffu : 0x100u;  // 0x100: no digit
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    uint32_t rank = __popc(peers & lanemask_lt);
-    bool leader = (peers & lanemask_lt) == 0;
-    if (valid && leader) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    // per digit: prefix over warps, then advance the digit base
-    {
-      int dd = tid;
-      uint32_t run = base[dd];
-#pragma unroll
-      for (int w = 0; w < 8; w++) {
-        uint32_t c = wcnt[w][dd];
-        wcnt[w][dd] = run;
-        run += c;
-      }
-      base[dd] = run;
+  // ---- place every item at its slot of the tile sorted by digit
+  for (int c = 0; c < kWarpItems / 32; c++) {
+    int j = warp * kWarpItems + c * 32 + lane;
+    int64_t i = tbase + j;
+    if (i < np) {
+      uint64_t k = kin[i];
+      uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+      uint32_t slot = lstart[d] + wc[warp][d] + rk[j];
+      sk[slot] = k;
+      sv[slot] = vin[i];
     }
-    __syncthreads();
-    if (valid) {
-      uint32_t dst = wcnt[warp][d] + rank;
-      kout[dst] = k;
-      vout[dst] = v;
-    }
-    __syncthreads();
+  }
+  __syncthreads();
+  // ---- write out: consecutive slots of a digit go to consecutive addresses
+  int64_t nt = np - tbase < kSortTile ? np - tbase : kSortTile;
+  for (int j = tid; j < nt; j += kSortThreads) {
+    uint64_t k = sk[j];
+    uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+    uint32_t g = gbase[d] + ((uint32_t)j - lstart[d]);
+    kout[g] = k;
+    vout[g] = sv[j];
   }
 }
+
+constexpr size_t kScatterSmem = (size_t)kSortTile * (8 + 4 + 2) + sizeof(uint32_t) * kScatterWarps * 256;
 
 void radix_sort_pairs(uint64_t **key, uint32_t **val, uint64_t *key_alt, uint32_t *val_alt,
                       int64_t np, int nbits, SortScratch &scr, cudaStream_t st, int64_t *launches) {
@@ -172,11 +210,16 @@ void radix_sort_pairs(uint64_t **key, uint32_t **val, uint64_t *key_alt, uint32_
   if (np <= 1) return;
   uint64_t *kin = *key, *kout = key_alt;
   uint32_t *vin = *val, *vout = val_alt;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem);
+    attr_set = true;
+  }
   for (int shift = 0; shift < nbits; shift += 8) {
     k_radix_hist<<<(unsigned)ntiles, kSortThreads, 0, st>>>(kin, np, shift, scr.hist, ntiles);
     k_radix_scan_digit<<<256, 1024, 0, st>>>(scr.hist, ntiles, scr.dtotal);
-    k_radix_scatter<<<(unsigned)ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, np, shift,
-                                                               scr.hist, scr.dtotal, ntiles);
+    k_radix_scatter<<<(unsigned)ntiles, kSortThreads, kScatterSmem, st>>>(kin, vin, kout, vout, np, shift,
+                                                                          scr.hist, scr.dtotal, ntiles);
     if (launches) *launches += 3;
     uint64_t *tk = kin;
     kin = kout;
