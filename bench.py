@@ -208,15 +208,23 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- engine arm
-def run_batched(args, E, ic, law, local):
+def run_batched(args, E, ic, law, local, dist=None):
     """The 64-box uneven ensemble: every box through the plain engine one
     after another (each call synchronises, as a caller of the plain engine
     does), then the same boxes as one ensemble (one graph launch per
-    evaluation). Both evaluate the same forces with the same law."""
+    evaluation). Both evaluate the same forces with the same law. With N
+    ranks every rank takes its share of the boxes (longest processing time
+    first); times are the max over ranks."""
     import torch
+    from lageunha_b200 import shard
+    ws = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    sizes = [ic.ensemble_spec(b)[0] ** 3 for b in range(args.ensemble_boxes)]
+    mine = shard.assign_boxes(sizes, ws)[rank]
     t0 = time.time()
-    boxes = ic.ensemble(args.ensemble_boxes)
+    boxes = [ic.ensemble_box(b) for b in mine]
     t_ic = time.time() - t0
+    dev = f"cuda:{local}"
     engines = [E.Engine(b.n_mesh, epsilon=EPS, device=local, **law) for b in boxes]
     for e, b in zip(engines, boxes):
         e.load_fixed(b.pos, b.vel)
@@ -248,12 +256,16 @@ def run_batched(args, E, ic, law, local):
     tp = []
     for _ in range(reps):
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         s = time.perf_counter()
         plain()
         tp.append(time.perf_counter() - s)
     tb, tbd = [], []
     for _ in range(reps):
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         s = time.perf_counter()
         batch.compute(E.PART_ALL)
         tb.append(time.perf_counter() - s)
@@ -267,7 +279,7 @@ def run_batched(args, E, ic, law, local):
     order = sorted(range(len(boxes)), key=lambda i: boxes[i].np)
     errs = []
     batch.compute(E.PART_ALL)
-    for i in (order[0], order[len(order) // 2], order[-1]):
+    for i in (sorted({order[0], order[len(order) // 2], order[-1]}) if order else []):
         b, e = boxes[i], engines[i]
         f = e.forces()
         rng = np.random.Generator(np.random.PCG64(1024 + i))
@@ -279,36 +291,48 @@ def run_batched(args, E, ic, law, local):
     batch.close()
     for e in engines:
         e.close()
-    plain_s, batch_s = min(tp), min(tb)
+    plain_s = shard.max_over_ranks(min(tp), dist, dev)
+    batch_s = shard.max_over_ranks(min(tb), dist, dev)
+    tbd_max = shard.max_over_ranks(min(tbd), dist, dev)
+    ms_step = shard.max_over_ranks(ms_step, dist, dev)
+    total = int(shard.sum_over_ranks(float(total), dist, dev))
     return {
-        "boxes": len(boxes), "particles": total,
-        "lattice_range": [min(b.n_lattice for b in boxes), max(b.n_lattice for b in boxes)],
-        "meshes": sorted({b.n_mesh for b in boxes}),
+        "boxes": args.ensemble_boxes, "boxes_per_rank": len(boxes), "particles": total,
+        "lattice_range": [min(ic.ensemble_spec(i)[0] for i in range(args.ensemble_boxes)),
+                          max(ic.ensemble_spec(i)[0] for i in range(args.ensemble_boxes))],
+        "meshes": sorted({ic.fft_friendly(ic.ensemble_spec(i)[0]) for i in range(args.ensemble_boxes)}),
         "plain_box_by_box": {"value": total / plain_s / 1e6, "ms": plain_s * 1e3},
-        "batched": {"value": total / batch_s / 1e6, "ms": batch_s * 1e3, "device_ms": min(tbd) * 1e3},
+        "batched": {"value": total / batch_s / 1e6, "ms": batch_s * 1e3, "device_ms": tbd_max * 1e3},
         "speedup": plain_s / batch_s,
         "kdk_step_ms": ms_step,
         "err_vs_ewald": errs,
         "ic_seconds": t_ic,
         "unit": UNIT,
-        "timing": "wall clock around each whole-ensemble evaluation after a device synchronize (best of 3); "
-                  "device_ms from CUDA events around the ensemble graph launch",
+        "timing": "wall clock around each whole-ensemble evaluation after a device synchronize (best of 3, "
+                  "max over ranks); device_ms from CUDA events around the ensemble graph launch",
     }
 
 
-def run_served(args, E, ic, law, local):
+def run_served(args, E, ic, law, local, dist=None):
     """Served solves: seeded Poisson arrivals (mean 200 requests/s) of boxes
     drawn log-uniform in 32^3..256^3 particles with 1-20 global steps each,
     submitted to the request loop at their arrival times; latency = done -
     arrival per request; throughput = particle-steps / (last done - first
     arrival)."""
+    from lageunha_b200 import shard
+    ws = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    dev = f"cuda:{local}"
     rng = np.random.Generator(np.random.PCG64(5))
     nreq = args.served_requests
     gaps = rng.exponential(1.0 / 200.0, nreq)
-    arrivals = np.cumsum(gaps) - gaps[0]
+    arrivals_all = np.cumsum(gaps) - gaps[0]
+    # request r goes to rank r mod N (one server per GPU)
+    mine = [r for r in range(nreq) if r % ws == rank]
+    arrivals = arrivals_all[mine]
     reqs = []
     t0 = time.time()
-    for r in range(nreq):
+    for r in mine:
         rr = np.random.Generator(np.random.PCG64(5000 + r))
         nl = int(round(np.exp(rr.uniform(np.log(32), np.log(256)))))
         nsteps = int(rr.integers(1, 21))
@@ -327,6 +351,8 @@ def run_served(args, E, ic, law, local):
     cosmo = E.cosmology()
     srv = E.Server(hbm_cap_bytes=150 * 10 ** 9, max_active=64, device=local)
     ids = []
+    if dist is not None:
+        dist.barrier()
     start = time.perf_counter()
     for r, ((box, nsteps), (pos, vel, po, vo)) in enumerate(zip(reqs, pinned)):
         delay = arrivals[r] - (time.perf_counter() - start)
@@ -346,6 +372,14 @@ def run_served(args, E, ic, law, local):
     span = max(i.t_done for i in infos) - min(i.t_submit for i in infos)
     work = sum(box.np * ns for box, ns in reqs)
     failed = sum(1 for i in infos if i.state != E.REQ_DONE)
+    if dist is not None and dist.get_world_size() > 1:
+        gathered = [None] * dist.get_world_size()
+        dist.all_gather_object(gathered, (lat.tolist(), wait.tolist()))
+        lat = np.array([x for g in gathered for x in g[0]])
+        wait = np.array([x for g in gathered for x in g[1]])
+        span = shard.max_over_ranks(span, dist, dev)
+        work = shard.sum_over_ranks(float(work), dist, dev)
+        failed = int(shard.sum_over_ranks(float(failed), dist, dev))
     return {
         "requests": nreq, "failed": failed, "arrival_rate_per_s": 200,
         "particle_steps": int(work), "value": work / span / 1e6, "unit": "Mparticle-steps/s",
@@ -576,9 +610,9 @@ def run_engine_arm(args):
     eng.close()
     box_law = REFERENCE_LAW if args.law == "reference" else BOX_LAW
     if not args.no_batched:
-        line["ensemble"] = {"law": box_law, **run_batched(args, E, ic, box_law, local)}
+        line["ensemble"] = {"law": box_law, **run_batched(args, E, ic, box_law, local, dist)}
     if not args.no_served:
-        line["served"] = {"law": box_law, **run_served(args, E, ic, box_law, local)}
+        line["served"] = {"law": box_law, **run_served(args, E, ic, box_law, local, dist)}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0:
