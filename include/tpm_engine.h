@@ -281,6 +281,31 @@ int tpm_server_stats(tpm_server *server, int64_t *out, int n);
 /* Finishes every submitted request, then stops the worker. */
 int tpm_server_destroy(tpm_server *server);
 
+/* ---- the reference's snapshot files ---- */
+
+/* What the ASCII header of a GOTPM snapshot says (FILE_HEADER,
+ * Params/params.h:500-517, written by jwrite, Cosmos/CosmosRW/kjhrw.c:169).
+ * ptype 0: dmparticletype records (32 bytes), 1: treedmparticletype (40). */
+typedef struct tpm_snapshot_info {
+  int64_t nx, ny, nz;
+  int64_t np_dm, np_sph, np_star, np_agn;
+  int32_t ptype, record_bytes;
+  double anow, astep;
+  float omep, omeplam, wlam0, wlam1, amax, boxsize, theta, epsilon, rsphere;
+  int32_t stepcount;
+  int64_t data_offset;  /* byte offset of the first dark-matter record */
+} tpm_snapshot_info;
+/* Parses the header (read_head, Params/header.c:72-104). */
+int tpm_snapshot_info_read(const char *path, tpm_snapshot_info *info);
+/* Reads dark-matter records [first, first + count) as they lie in the file
+ * (record_bytes each); they load with tpm_load_lagrangian. */
+int tpm_snapshot_read_dm(const char *path, const tpm_snapshot_info *info, void *records, int64_t first,
+                         int64_t count);
+/* Writes a snapshot the reference's jread accepts: the header lines in the
+ * reference's key formats and np_dm dark-matter records (no other species,
+ * no trailing parameter struct: jread then decomposes the domain itself). */
+int tpm_snapshot_write(const char *path, const tpm_snapshot_info *info, const void *dm_records);
+
 /* ---- diagnostics ---- */
 
 /* FP64 periodic Ewald force (reference units, Plummer softening epsilon on

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtpm_engine.so")
-SOURCES = ["engine.cu", "sort.cu", "pm.cu", "tree.cu", "ewald.cu", "noalloc.cu", "step.cu", "batch.cu", "server.cu", "tune.cu"]
+SOURCES = ["engine.cu", "sort.cu", "pm.cu", "tree.cu", "ewald.cu", "noalloc.cu", "step.cu", "batch.cu", "server.cu", "tune.cu", "snapshot.cpp"]
 HEADERS = ["common.cuh", "engine_internal.cuh", "ctx.cuh"]
 
 NVCC_FLAGS = [
@@ -48,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     objs = []
     for src in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))

@@ -83,6 +83,16 @@ class TpmTuning(ctypes.Structure):
 TUNE_FFT, TUNE_GROUPS = 1, 2
 
 
+class TpmSnapshotInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("nz", ctypes.c_int64), ("np_dm", ctypes.c_int64),
+                ("np_sph", ctypes.c_int64), ("np_star", ctypes.c_int64), ("np_agn", ctypes.c_int64),
+                ("ptype", ctypes.c_int32), ("record_bytes", ctypes.c_int32), ("anow", ctypes.c_double),
+                ("astep", ctypes.c_double)] + \
+        [(k, ctypes.c_float) for k in ("omep", "omeplam", "wlam0", "wlam1", "amax", "boxsize", "theta", "epsilon",
+                                       "rsphere")] + \
+        [("stepcount", ctypes.c_int32), ("data_offset", ctypes.c_int64)]
+
+
 class EngineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"tpm error {code}: {msg}")
@@ -133,6 +143,9 @@ _SIGS = {
     "tpm_autotune": (ctypes.c_int, [_P, ctypes.c_uint, ctypes.POINTER(TpmTuning)]),
     "tpm_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
     "tpm_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
+    "tpm_snapshot_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo)]),
+    "tpm_snapshot_read_dm": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo), _P, _I64, _I64]),
+    "tpm_snapshot_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo), _P]),
     "tpm_estimate_bytes": (ctypes.c_int64, [ctypes.c_int32, ctypes.c_int64]),
     "tpm_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     "tpm_server_submit": (ctypes.c_int, [_P, ctypes.POINTER(TpmRequest), ctypes.POINTER(ctypes.c_int64)]),
@@ -506,6 +519,35 @@ def evol_factors(cosmo: TpmCosmology, nx: int, anow: float, astep: float) -> dic
     out = TpmEvolFact()
     _check(load_library().tpm_evol_factors(ctypes.byref(cosmo), nx, anow, astep, ctypes.byref(out)))
     return {k: getattr(out, k) for k, _ in TpmEvolFact._fields_}
+
+
+def read_snapshot(path: str):
+    """(header dict, dark-matter records) of a GOTPM snapshot file: records as
+    DM_DTYPE (particle type 0) or TREEDM_DTYPE (1), ready for
+    Engine.load_lagrangian."""
+    lib = load_library()
+    info = TpmSnapshotInfo()
+    _check(lib.tpm_snapshot_info_read(path.encode(), ctypes.byref(info)))
+    rec = np.empty(info.np_dm, DM_DTYPE if info.ptype == 0 else TREEDM_DTYPE)
+    _check(lib.tpm_snapshot_read_dm(path.encode(), ctypes.byref(info), rec.ctypes.data, 0, info.np_dm))
+    return {k: getattr(info, k) for k, _ in TpmSnapshotInfo._fields_}, rec
+
+
+def write_snapshot(path: str, records: np.ndarray, n_mesh: int, **header):
+    """A GOTPM snapshot of the records (DM_DTYPE or TREEDM_DTYPE) that the
+    reference's jread reads; header: omep, omeplam, wlam0, wlam1, amax, anow,
+    astep, boxsize, theta, epsilon, stepcount."""
+    lib = load_library()
+    info = TpmSnapshotInfo()
+    info.nx = info.ny = info.nz = n_mesh
+    info.np_dm = records.shape[0]
+    info.ptype = 0 if records.dtype == DM_DTYPE else 1
+    info.omep, info.omeplam, info.wlam0, info.wlam1, info.amax = 0.26, 0.74, -1.0, 0.0, 48.0
+    info.anow, info.astep, info.boxsize, info.theta, info.epsilon = 1.0, 0.02, 100.0, 0.3, 0.1
+    for k, v in header.items():
+        setattr(info, k, v)
+    rec = np.ascontiguousarray(records)
+    _check(lib.tpm_snapshot_write(path.encode(), ctypes.byref(info), rec.ctypes.data))
 
 
 def dm_records(ps) -> np.ndarray:

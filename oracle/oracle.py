@@ -70,6 +70,9 @@ def ref(variant: int = VARIANT_B):
         L.ref_potential.argtypes = [_int, _i64, _u64p, _f32p, _flt, _f32p]
         L.ref_spline_table.argtypes = [_int, _flt, _f64p, _f64p]
         L.ref_evol_factors.argtypes = [_int, _flt, _flt, _flt, _flt, _flt, _flt, _flt, _f32p]
+        L.ref_write_snapshot.argtypes = [ctypes.c_char_p, _int, ctypes.c_int64, ctypes.c_void_p] + [_flt] * 5 + \
+            [ctypes.c_double] * 2 + [_flt] * 4 + [_int]
+        L.ref_read_head.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
         _ref[variant] = L
     return _ref[variant]
 
@@ -182,6 +185,28 @@ def ref_evol_factors(n, omep, omeplam, wlam0, wlam1, amax, anow, astep):
     out = np.zeros(9, np.float32)
     ref(VARIANT_A).ref_evol_factors(n, omep, omeplam, wlam0, wlam1, amax, anow, astep, out)
     return dict(zip(EVOL_FIELDS, out))
+
+
+SNAPSHOT_FIELDS = ("nx", "ny", "nz", "np_dm", "np_sph", "np_star", "np_agn", "ptype", "omep", "omeplam", "wlam0",
+                   "wlam1", "amax", "anow", "astep", "theta", "epsilon", "rsphere", "boxsize", "stepcount")
+
+
+def ref_write_snapshot(path, n, records, omep=0.26, omeplam=0.74, wlam0=-1.0, wlam1=0.0, amax=48.0, anow=1.0,
+                       astep=0.02, boxsize=100.0, theta=0.3, eps=0.05, rsphere=4.0, stepcount=0):
+    """One rank's GOTPM snapshot as the reference's jwrite writes it."""
+    rec = np.ascontiguousarray(records)
+    rc = ref(VARIANT_A).ref_write_snapshot(path.encode(), n, rec.shape[0], rec.ctypes.data, omep, omeplam, wlam0,
+                                           wlam1, amax, anow, astep, boxsize, theta, eps, rsphere, stepcount)
+    if rc != rec.dtype.itemsize:
+        raise RuntimeError(f"reference record size {rc} != {rec.dtype.itemsize}")
+
+
+def ref_read_head(path):
+    """The header of a snapshot as the reference's read_head parses it."""
+    out = np.zeros(len(SNAPSHOT_FIELDS), np.float64)
+    if ref(VARIANT_A).ref_read_head(path.encode(), out.ctypes.data) != 0:
+        raise RuntimeError(f"cannot read {path}")
+    return dict(zip(SNAPSHOT_FIELDS, out))
 
 
 def rel_err(f, fref):

@@ -413,3 +413,78 @@ int ref_evol_factors(int n, float omep, float omeplam, float wlam0, float wlam1,
   free(b);
   return 0;
 }
+
+/* ------------------------------------------------------ snapshot files */
+/* Mpi_Basic_Set (MpiAux) is named by Params/header.c but not reached by
+ * read_head / write_head. */
+void Mpi_Basic_Set(SimParameters *s, MPI_Comm comm) {
+  (void)s;
+  (void)comm;
+  fprintf(stderr, "oracle/_ref: Mpi_Basic_Set is not part of the oracle harness\n");
+  abort();
+}
+void write_head(FILE *, SimParameters *);
+void read_head(FILE *, SimParameters *);
+void mk_default_param(SimParameters *, char *);
+
+/* One rank's file as jwrite writes it (Cosmos/CosmosRW/kjhrw.c:196-211, GOTPM
+ * PMTYPE): write_head, the dmparticletype records (32 bytes each), then the
+ * SimParameters struct. */
+int ref_write_snapshot(const char *path, int n, int64_t np, const void *records, float omep, float omeplam,
+                       float wlam0, float wlam1, float amax, double anow, double astep, float boxsize,
+                       float theta, float eps, float rsphere, int stepcount) {
+  SimParameters *s = (SimParameters *)calloc(1, sizeof(SimParameters));
+  mk_default_param(s, (char *)"WMAP5");
+  MYID(s) = 0;
+  NID(s) = 1;
+  NX(s) = NY(s) = NZ(s) = n;
+  NXNY(s) = (ptrdiff_t)n * n;
+  OMEP(s) = omep;
+  OMEPLAM(s) = omeplam;
+  WLAM0(s) = wlam0;
+  WLAM1(s) = wlam1;
+  AMAX(s) = amax;
+  ANOW(s) = anow;
+  ASTEP(s) = astep;
+  COSBOXSIZE(s) = boxsize;
+  THETA(s) = theta;
+  GRV_EPSILON(s) = eps;
+  RSPHERE(s) = rsphere;
+  STEPCOUNT(s) = stepcount;
+  DM_NP(s) = np;
+  NPSUM(s) = np;
+  PTYPE(s) = PMTYPE;
+  FILE *fp = fopen(path, "w");
+  if (!fp) {
+    free(s);
+    return -1;
+  }
+  write_head(fp, s);
+  fwrite(records, sizeof(dmparticletype), (size_t)np, fp);
+  fwrite(s, sizeof(SimParameters), 1, fp);
+  fclose(fp);
+  free(s);
+  return (int)sizeof(dmparticletype);
+}
+
+/* read_head of a file (Params/header.c:72-104): the fields the engine's
+ * reader reports, in this order: nx ny nz np_dm np_sph np_star np_agn ptype
+ * omep omeplam wlam0 wlam1 amax anow astep theta epsilon rsphere boxsize
+ * stepcount. */
+int ref_read_head(const char *path, double *out) {
+  SimParameters *s = (SimParameters *)calloc(1, sizeof(SimParameters));
+  FILE *fp = fopen(path, "r");
+  if (!fp) {
+    free(s);
+    return -1;
+  }
+  read_head(fp, s);
+  fclose(fp);
+  double v[20] = {(double)NX(s), (double)NY(s), (double)NZ(s), (double)DM_NP(s), (double)SPH_NP(s),
+                  (double)STAR_NP(s), (double)AGN_NP(s), (double)PTYPE(s), OMEP(s), OMEPLAM(s), WLAM0(s),
+                  WLAM1(s), AMAX(s), ANOW(s), ASTEP(s), THETA(s), GRV_EPSILON(s), RSPHERE(s),
+                  COSBOXSIZE(s), (double)STEPCOUNT(s)};
+  memcpy(out, v, sizeof(v));
+  free(s);
+  return 0;
+}
