@@ -281,6 +281,22 @@ int tpm_server_stats(tpm_server *server, int64_t *out, int n);
 /* Finishes every submitted request, then stops the worker. */
 int tpm_server_destroy(tpm_server *server);
 
+/* ---- power spectrum of the mass assignment ---- */
+
+/* With it enabled, every PM evaluation also bins |rho_k|^2 of the forward
+ * transform, as the reference's CorrMeasure does after pmmain's forward FFT
+ * (Cosmos/pmmain.c:480-481, Cosmos/Correlation.c:13-79): TSC window divided
+ * out, kx < N/2, linear sharing between the bins floor(|m|) and its
+ * neighbour. Costs one pass of bin additions inside the z transform. */
+int tpm_set_power_spectrum(tpm_ctx *ctx, int enable);
+/* From the last PM evaluation: P(k) per bin (bin i = |m| in mode numbers,
+ * i = 1..N, bin 0 as accumulated), the correlation function xi at i cells,
+ * sigma_8 for the box size in Mpc/h and the log slope of xi between 2 and 3
+ * cells (Correlation.c:82-103). Fills min(nbins, N+1) entries and returns
+ * that count. */
+int tpm_power_spectrum(tpm_ctx *ctx, double boxsize, double *pk, double *cor, int32_t nbins, double *sigma8,
+                       double *slope);
+
 /* ---- the reference's snapshot files ---- */
 
 /* What the ASCII header of a GOTPM snapshot says (FILE_HEADER,

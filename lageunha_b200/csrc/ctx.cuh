@@ -76,6 +76,9 @@ struct tpm_ctx {
   float law_eps = -1, law_rs = -1, law_rsphere = -1;
   int law_kind = -1;
   uint32_t *err = nullptr;
+  // power spectrum of the mass assignment (tpm_set_power_spectrum)
+  bool measure_pk = false;
+  double *pk_acc = nullptr;  // device [2][n+1]
   // launch shapes (tpm_autotune): 0 = the built-in choice
   int tune_fft_px = 0, tune_fft_tx = 0;
   int tune_group_level = 2;  // groups live in cubes of 2^level cells

@@ -259,6 +259,9 @@ static int ensure_mesh2(tpm_ctx *c) {
 
 static void free_mesh(tpm_ctx *c) {
   free_mesh2(c);
+  if (c->pk_acc) cudaFree(c->pk_acc);
+  c->pk_acc = nullptr;
+  c->measure_pk = false;
   if (c->rho) cudaFree(c->rho);
   if (c->spec) cudaFree(c->spec);
   if (c->phi) cudaFree(c->phi);
@@ -728,12 +731,14 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     c->launches += 2;
     CK(stage_check(st, "deposit"));
     if (timing) CK(cudaEventRecord(c->ev[2], st));
+    double *pk = c->measure_pk ? c->pk_acc : nullptr;
+    if (pk) CK(cudaMemsetAsync(pk, 0, sizeof(double) * 2 * (g.n + 1), st));
     if (il)
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
-                     &c->launches, c->rho2, c->spec2, c->phi2, c->gt, c->tune_fft_px, c->tune_fft_tx);
+                     &c->launches, c->rho2, c->spec2, c->phi2, c->gt, c->tune_fft_px, c->tune_fft_tx, pk);
     else
       launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
-                     &c->launches, nullptr, nullptr, nullptr, nullptr, c->tune_fft_px, c->tune_fft_tx);
+                     &c->launches, nullptr, nullptr, nullptr, nullptr, c->tune_fft_px, c->tune_fft_tx, pk);
     CK(stage_check(st, "fft"));
     if (timing) CK(cudaEventRecord(c->ev[3], st));
     // the reference law keeps the reference's 4-point gradient; the Gaussian

@@ -75,7 +75,8 @@ void fft_plan_free(FftPlan &p);
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
                     int64_t *launches, const float *rho2 = nullptr, float2 *spec2 = nullptr,
-                    float *phi2_pad = nullptr, const float *gt = nullptr, int want_px = 0, int want_tx = 0);
+                    float *phi2_pad = nullptr, const float *gt = nullptr, int want_px = 0, int want_tx = 0,
+                    double *pk = nullptr);
 // The optimal influence function of the interlaced pair with the 8-point
 // gradient for split scale rs, [ky][kx][kz] with kx < n/2 + 1.
 void launch_green_opt(float *gt, int n, double rs, cudaStream_t st);

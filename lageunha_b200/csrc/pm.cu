@@ -491,7 +491,41 @@ struct GreenArgs {
   float rs2k;    // gaussian law: (2 pi rs / n)^2
   int n;
   const float *gt;  // tabulated influence function [ky][kx][kz] (interlaced grids), or null
+  double *pk;       // power-spectrum bins [2][n+1] (sum of weights*|rho_k|^2, sum of weights), or null
 };
+
+// The reference's CorrMeasure (Cosmos/Correlation.c:13-79) on the forward
+// spectrum of the first grid: for kx < n/2, |rho_k|^2 / n^6 divided by the
+// squared TSC window, shared linearly between the bins floor(|m|) and its
+// neighbour towards |m|. Bins are summed per block in shared memory (sbin,
+// 2(n+1) floats) and added to the device totals in double.
+TPM_D void pk_accumulate(float *sbin, int n, int kx, int wy, int wz, float2 v) {
+  if (2 * kx >= n) return;
+  float wave = sqrtf((float)(kx * kx + wy * wy + wz * wz));
+  float conv = 1.f;
+  int ks[3] = {kx, wy, wz};
+  for (int d = 0; d < 3; d++) {
+    if (ks[d] != 0) {
+      float a = (float)ks[d] / (float)n;
+      float sc = sinpif(a) / (3.14159265358979323846f * a);
+      conv *= sc * sc * sc;
+    }
+  }
+  float inv_n3 = 1.f / ((float)n * (float)n * (float)n);
+  float re = v.x * inv_n3, im = v.y * inv_n3;
+  float d = (re * re + im * im) / (conv * conv);
+  int k1 = (int)wave;
+  float w = wave - (float)k1;
+  int k2 = k1 + (w > 0.f ? 1 : -1);
+  if (k1 <= n) {
+    atomicAdd(&sbin[k1], (1.f - w) * d);
+    atomicAdd(&sbin[n + 1 + k1], 1.f - w);
+  }
+  if (k2 >= 0 && k2 <= n && w > 0.f) {
+    atomicAdd(&sbin[k2], w * d);
+    atomicAdd(&sbin[n + 1 + k2], w);
+  }
+}
 
 TPM_D float green(const GreenArgs &g, int kx, int ky, int kz) {
   float wy = (float)ky, wz = (float)kz;
@@ -549,6 +583,19 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, P, dir, a.radix, a.nf);
+  if (with_green && ga.pk) {
+    float *sbin = reinterpret_cast<float *>(B + P * L);
+    for (int e = tid; e < 2 * (n + 1); e += nth) sbin[e] = 0.f;
+    __syncthreads();
+    int wy = outer > n / 2 ? outer - n : outer;
+    for (int e = tid; e < TX * L; e += nth) {
+      int q = e / L, m = e - q * L;
+      if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[e]);
+    }
+    __syncthreads();
+    for (int e = tid; e < 2 * (n + 1); e += nth)
+      if (sbin[e] != 0.f) atomicAdd(&ga.pk[e], (double)sbin[e]);
+  }
   if (with_green) {
     if (nspec == 1) {
       for (int e = tid; e < P * L; e += nth) {
@@ -674,7 +721,8 @@ static int pencils_for(int L, int want = 0) {
 // nspec * TX pencils) would exceed 160 KB.
 static int cols_per_block(int n, int hx, int nspec, int want = 0) {
   int TX = want > 0 ? want : (n >= 256 ? 8 : 16);
-  int tmax = (int)(((160 * 1024) / (int)sizeof(float2) / n - 1) / (2 * nspec));
+  // room for the power-spectrum bins (2(n+1) floats) as well
+  int tmax = (int)(((160 * 1024 - 8 * (n + 1)) / (int)sizeof(float2) / n - 1) / (2 * nspec));
   if (TX > tmax) TX = tmax;
   if (TX > hx) TX = hx;
   if (TX < 1) TX = 1;
@@ -745,7 +793,7 @@ void launch_green_opt(float *gt, int n, double rs, cudaStream_t st) {
 void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float2 *spec,
                     float *phi_pad, int law, float efold, float rs_split, cudaStream_t st,
                     int64_t *launches, const float *rho2, float2 *spec2, float *phi2_pad, const float *gt,
-                    int want_px, int want_tx) {
+                    int want_px, int want_tx, double *pk) {
   int n = g.n;
   int64_t nrows = (int64_t)n * n;
   bool packed = (n % 2) == 0;
@@ -761,7 +809,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   // columns
   int TX = cols_per_block(n, g.hx, nspec, want_tx);
   FftArgs ac = fft_args(n, n, TX * nspec);
-  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * n);
+  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * n) + (pk ? sizeof(float) * 2 * (n + 1) : 0);
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   ga.law = law;
@@ -770,6 +818,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   ga.irngc = (float)(1.0 / ((double)n * n * n));
   ga.rs2k = (float)pow(2.0 * M_PI * (double)rs_split / (double)n, 2);
   ga.gt = rho2 ? gt : nullptr;
+  ga.pk = pk;
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, -1.f, 0, ga, TX, nspec);
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 2, -1.f, 1, ga, TX, nspec);
   k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, spec2, ac, p.tw, 1, 1.f, 0, ga, TX, nspec);

@@ -143,6 +143,8 @@ _SIGS = {
     "tpm_autotune": (ctypes.c_int, [_P, ctypes.c_uint, ctypes.POINTER(TpmTuning)]),
     "tpm_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
     "tpm_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
+    "tpm_set_power_spectrum": (ctypes.c_int, [_P, ctypes.c_int]),
+    "tpm_power_spectrum": (ctypes.c_int, [_P, ctypes.c_double, _P, _P, ctypes.c_int32, _P, _P]),
     "tpm_snapshot_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo)]),
     "tpm_snapshot_read_dm": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo), _P, _I64, _I64]),
     "tpm_snapshot_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo), _P]),
@@ -350,6 +352,22 @@ class Engine:
     @tuning.setter
     def tuning(self, t: TpmTuning):
         _check(self._lib.tpm_set_tuning(self._ctx, ctypes.byref(t)))
+
+    def measure_power_spectrum(self, enable: bool = True):
+        _check(self._lib.tpm_set_power_spectrum(self._ctx, 1 if enable else 0))
+
+    def power_spectrum(self, boxsize: float) -> dict:
+        """P(k), xi, sigma_8 and the xi slope of the last PM evaluation
+        (the reference's CorrMeasure)."""
+        nb = self.n_mesh + 1
+        pk = np.zeros(nb)
+        cor = np.zeros(nb)
+        s8 = ctypes.c_double()
+        sl = ctypes.c_double()
+        k = self._lib.tpm_power_spectrum(self._ctx, boxsize, pk.ctypes.data, cor.ctypes.data, nb,
+                                         ctypes.addressof(s8), ctypes.addressof(sl))
+        _check(k if k < 0 else 0)
+        return {"pk": pk[:k], "cor": cor[:k], "sigma8": s8.value, "slope": sl.value}
 
     def hubble_drag(self, fact1: float):
         _check(self._lib.tpm_hubble_drag(self._ctx, fact1))

@@ -73,6 +73,8 @@ def ref(variant: int = VARIANT_B):
         L.ref_write_snapshot.argtypes = [ctypes.c_char_p, _int, ctypes.c_int64, ctypes.c_void_p] + [_flt] * 5 + \
             [ctypes.c_double] * 2 + [_flt] * 4 + [_int]
         L.ref_read_head.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+        L.ref_power_spectrum.argtypes = [_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                         ctypes.c_void_p]
         _ref[variant] = L
     return _ref[variant]
 
@@ -207,6 +209,32 @@ def ref_read_head(path):
     if ref(VARIANT_A).ref_read_head(path.encode(), out.ctypes.data) != 0:
         raise RuntimeError(f"cannot read {path}")
     return dict(zip(SNAPSHOT_FIELDS, out))
+
+
+def ref_power_spectrum(n, indx, off, boxsize):
+    """The reference's CorrMeasure (Cosmos/Correlation.c) on one pmmain of
+    the particles: {"pk": P(k) for bins 0..N/2-1, "cor": xi at 0..N/2-1 cells,
+    "sigma8", "slope"}, parsed from the pmevol.map it writes (7 significant
+    digits)."""
+    import os
+    import tempfile
+    idx = np.ascontiguousarray(indx, np.uint64)
+    o = np.ascontiguousarray(off, np.float32)
+    force = np.zeros((idx.shape[0], 3), np.float32)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as d:
+        os.chdir(d)
+        try:
+            ref(VARIANT_A).ref_power_spectrum(n, idx.shape[0], idx.ctypes.data, o.ctypes.data, boxsize,
+                                              force.ctypes.data)
+            lines = open("pmevol.map").read().split("\n")
+        finally:
+            os.chdir(cwd)
+    anow, s8, slope = (float(x) for x in lines[0].split())
+    rows = [l.split() for l in lines[1:] if l.strip()]
+    pk = np.array([float(r[2]) for r in rows])
+    cor = np.array([float(r[3]) for r in rows])
+    return {"pk": pk, "cor": cor, "sigma8": s8, "slope": slope}
 
 
 def rel_err(f, fref):

@@ -197,7 +197,18 @@ void PaddingParticles(SimParameters *simpar) {
 }
 
 /* ---------------------------------------------- skipped side effects */
-void CorrMeasure(SimParameters *simpar, GridInfo *g) { (void)simpar; (void)g; }
+/* pmmain calls CorrMeasure after its forward FFT (Cosmos/pmmain.c:480-481);
+ * the reference's own function (compiled as ref_corr_measure) runs only
+ * when ref_power_spectrum asks for it, and writes pmevol.map in the current
+ * directory. */
+void ref_corr_measure(SimParameters *simpar, GridInfo *g);
+static int g_corr = 0;
+static double g_corr_boxsize = 0;
+void CorrMeasure(SimParameters *simpar, GridInfo *g) {
+  if (!g_corr) return;
+  BOXSIZE(simpar) = g_corr_boxsize;
+  ref_corr_measure(simpar, g);
+}
 void savexzslice(SimParameters *simpar, DenType *d) { (void)simpar; (void)d; }
 void volumeout(SimParameters *simpar, GridInfo *g, int which) { (void)simpar; (void)g; (void)which; }
 
@@ -487,4 +498,15 @@ int ref_read_head(const char *path, double *out) {
   memcpy(out, v, sizeof(v));
   free(s);
   return 0;
+}
+
+/* The reference's P(k) of a particle set: one pmmain with CorrMeasure on
+ * (Cosmos/Correlation.c:13-117); its output is the pmevol.map file it writes
+ * in the current directory. */
+int ref_power_spectrum(int n, int64_t np, const uint64_t *indx, const float *off, double boxsize, float *force) {
+  g_corr = 1;
+  g_corr_boxsize = boxsize;
+  int rc = ref_pm_force(n, np, indx, off, 0.9f, force);
+  g_corr = 0;
+  return rc;
 }
