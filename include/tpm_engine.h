@@ -297,6 +297,17 @@ int tpm_set_power_spectrum(tpm_ctx *ctx, int enable);
 int tpm_power_spectrum(tpm_ctx *ctx, double boxsize, double *pk, double *cor, int32_t nbins, double *sigma8,
                        double *slope);
 
+/* ---- friends-of-friends groups ---- */
+
+/* Groups of particles linked by distance <= link (cells), as the reference's
+ * pnew_fof_link grows them (FoF/fof.c:217-290; PreFoF, Cosmos/PreFoF.c:
+ * 267-385, uses link 0.2 and at least 20 members). labels[i] (caller order)
+ * is the smallest caller index of particle i's group if the group has at
+ * least min_members particles, else -1; *ngroups counts those groups. Uses
+ * the sort and octree of a force evaluation; the forces held before are
+ * dropped. */
+int tpm_fof(tpm_ctx *ctx, float link, int32_t min_members, int32_t *labels, int mem, int64_t *ngroups);
+
 /* ---- the reference's snapshot files ---- */
 
 /* What the ASCII header of a GOTPM snapshot says (FILE_HEADER,

@@ -143,6 +143,7 @@ _SIGS = {
     "tpm_autotune": (ctypes.c_int, [_P, ctypes.c_uint, ctypes.POINTER(TpmTuning)]),
     "tpm_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
     "tpm_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(TpmTuning)]),
+    "tpm_fof": (ctypes.c_int, [_P, ctypes.c_float, ctypes.c_int32, _P, ctypes.c_int, _P]),
     "tpm_set_power_spectrum": (ctypes.c_int, [_P, ctypes.c_int]),
     "tpm_power_spectrum": (ctypes.c_int, [_P, ctypes.c_double, _P, _P, ctypes.c_int32, _P, _P]),
     "tpm_snapshot_info_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(TpmSnapshotInfo)]),
@@ -352,6 +353,14 @@ class Engine:
     @tuning.setter
     def tuning(self, t: TpmTuning):
         _check(self._lib.tpm_set_tuning(self._ctx, ctypes.byref(t)))
+
+    def fof(self, link: float = 0.2, min_members: int = 20):
+        """(labels, ngroups): friends-of-friends groups of the loaded
+        particles; labels[i] = smallest caller index of i's group or -1."""
+        out = np.empty(self.np, np.int32)
+        ng = ctypes.c_int64()
+        _check(self._lib.tpm_fof(self._ctx, link, min_members, out.ctypes.data, MEM_HOST, ctypes.addressof(ng)))
+        return out, ng.value
 
     def measure_power_spectrum(self, enable: bool = True):
         _check(self._lib.tpm_set_power_spectrum(self._ctx, 1 if enable else 0))

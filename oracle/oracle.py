@@ -237,6 +237,26 @@ def ref_power_spectrum(n, indx, off, boxsize):
     return {"pk": pk, "cor": cor, "sigma8": s8, "slope": slope}
 
 
+def fof_labels(n, pos, link, min_members):
+    """Friends-of-friends groups (FoF/fof.c:217-290: particles linked when
+    their distance is <= link; the groups are the connected components of
+    that relation) in FP64 with periodic minimum images: label = smallest
+    particle index of the group if it has >= min_members particles, else -1."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    from scipy.spatial import cKDTree
+    p = np.mod(np.asarray(pos, np.float64), n)
+    pairs = cKDTree(p, boxsize=float(n)).query_pairs(r=link, output_type="ndarray")
+    m = p.shape[0]
+    g = coo_matrix((np.ones(len(pairs)), (pairs[:, 0], pairs[:, 1])), shape=(m, m))
+    _, comp = connected_components(g, directed=False)
+    size = np.bincount(comp)
+    first = np.full(comp.max() + 1, m, np.int64)
+    np.minimum.at(first, comp, np.arange(m))
+    lab = np.where(size[comp] >= min_members, first[comp], -1)
+    return lab.astype(np.int64), int(np.sum(size >= min_members))
+
+
 def rel_err(f, fref):
     """Per-particle |f - fref| / |fref|."""
     num = np.linalg.norm(np.asarray(f, np.float64) - np.asarray(fref, np.float64), axis=1)
