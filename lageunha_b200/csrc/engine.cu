@@ -190,9 +190,39 @@ static int build_law(tpm_ctx *c) {
       tlog[k] = make_float2((float)v[k], (float)((v[k + 1] - v[k]) * (double)(1 << kLogMantissa)));
     tlog[kLogEntries] = make_float2(0.f, 0.f);
   }
+  // the node terms' derivative columns on the coarse log grid, with the same
+  // central differences as the linear table
+  std::vector<float4> tpc(kPcEntries + 1);
+  {
+    std::vector<double> f2(kPcEntries + 1), f3(kPcEntries + 1);
+    double rs2 = (double)p.rsphere * (double)p.rsphere;
+    for (int k = 0; k <= kPcEntries; k++) {
+      uint32_t bits = (uint32_t)(kPcBase + k) << kPcShift;
+      float sf;
+      memcpy(&sf, &bits, 4);
+      double s = (double)sf, r = sqrt(s);
+      if (s >= rs2) {
+        f2[k] = f3[k] = 0.0;
+        continue;
+      }
+      double fp = (law_f(p.law, r + dr, p.epsilon, p.rs_split, LL) - law_f(p.law, r - dr, p.epsilon, p.rs_split, LL)) / (dr + dr);
+      double fpp = (law_f(p.law, r + 2 * dr, p.epsilon, p.rs_split, LL) - 2 * law_f(p.law, r, p.epsilon, p.rs_split, LL) +
+                    law_f(p.law, r - 2 * dr, p.epsilon, p.rs_split, LL)) / (4 * dr * dr);
+      double fr = law_f(p.law, r, p.epsilon, p.rs_split, LL);
+      f2[k] = -(0.5 * (fp * r - fr) / r / r / r);
+      f3[k] = -(0.5 * (fpp * r * r - 3 * fp * r + 3 * fr) / r / r / r / r / r);
+    }
+    const double sc = (double)(1 << kPcMantissa);
+    for (int k = 0; k < kPcEntries; k++)
+      tpc[k] = make_float4((float)f2[k], (float)((f2[k + 1] - f2[k]) * sc), (float)f3[k],
+                           (float)((f3[k + 1] - f3[k]) * sc));
+    tpc[kPcEntries] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   if (c->law.t0 || c->law.t12) CK(cudaStreamSynchronize(c->st));
   if (c->law.tlog) cudaFree(c->law.tlog);
+  if (c->law.tpc) cudaFree(c->law.tpc);
   c->law.tlog = nullptr;
+  c->law.tpc = nullptr;
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
   c->law.t0 = nullptr;
@@ -203,6 +233,8 @@ static int build_law(tpm_ctx *c) {
   CK(cudaMemcpy(c->law.t12, t12.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c->law.tlog, sizeof(float2) * (kLogEntries + 1)));
   CK(cudaMemcpy(c->law.tlog, tlog.data(), sizeof(float2) * (kLogEntries + 1), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->law.tpc, sizeof(float4) * (kPcEntries + 1)));
+  CK(cudaMemcpy(c->law.tpc, tpc.data(), sizeof(float4) * (kPcEntries + 1), cudaMemcpyHostToDevice));
   c->law.entries = entries;
   c->law.hard_cut = hard_cut;
   c->law.delta = ran2nran;
@@ -598,6 +630,7 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->law.t0) cudaFree(c->law.t0);
   if (c->law.t12) cudaFree(c->law.t12);
   if (c->law.tlog) cudaFree(c->law.tlog);
+  if (c->law.tpc) cudaFree(c->law.tpc);
   if (c->err) cudaFree(c->err);
   if (c->tb.counters) cudaFree(c->tb.counters);
   if (c->tb.level_range) cudaFree(c->tb.level_range);

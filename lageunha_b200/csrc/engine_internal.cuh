@@ -153,10 +153,18 @@ constexpr int kLogMantissa = 7;
 constexpr int kLogShift = 23 - kLogMantissa;
 constexpr int kLogBase = (127 - 20) << kLogMantissa;
 constexpr int kLogEntries = 26 << kLogMantissa;
+// The node terms' derivative columns (f2, f3 of the linear table t12) on a
+// coarser log grid of r^2, 2^kPcMantissa bins per octave from 2^-8 to 2^6
+// cells^2 (accepted nodes are never closer): {f2, df2 * 2^m, f3, df3 * 2^m}.
+constexpr int kPcMantissa = 5;
+constexpr int kPcShift = 23 - kPcMantissa;
+constexpr int kPcBase = (127 - 8) << kPcMantissa;
+constexpr int kPcEntries = 14 << kPcMantissa;
 struct LawTable {
   float2 *t0 = nullptr;
   float4 *t12 = nullptr;
   float2 *tlog = nullptr;  // [kLogEntries + 1]
+  float4 *tpc = nullptr;   // [kPcEntries + 1]
   int entries = 0;
   float delta = 0, inv_delta = 0;
   // 1: the walk tests r <= rsphere per pair (the reference's cut);

@@ -595,8 +595,7 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 // and z components on their own axes. Coordinates are in cells; the linear
 // tables (t0, t12, index w = r / delta) give the law and its derivatives.
 TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpu, float rs2,
-                   const float2 *__restrict__ t0, const float4 *__restrict__ t12, float inv_delta,
-                   float wmax, unsigned long long &npc) {
+                   const float2 *__restrict__ tl, const float4 *__restrict__ tq, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
   for (int base = 0; base < m_all; base += 32) {
     int m = min(32, m_all - base);
@@ -615,12 +614,16 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, floa
       float4 c0 = wl.stage[3 * j], q1 = wl.stage[3 * j + 1], q2 = wl.stage[3 * j + 2];
       float dx = w.tx - c0.x, dy = w.ty - c0.y, dz = w.tz - c0.z;
       float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float wq = fminf(r2 * rsqrt_approx(r2) * inv_delta, wmax);
-      float frac;
-      int nt = table_index(wq, frac);
-      float2 c = __ldg(&t0[nt]);
-      float4 d = __ldg(&t12[nt]);
-      float f1 = fmaf(c.y, frac, c.x), f2 = fmaf(d.y, frac, d.x), f3 = fmaf(d.w, frac, d.z);
+      // f1 from the particle-particle table, f2 and f3 from the coarse one,
+      // both indexed by the bits of r^2 (shared memory)
+      uint32_t bits = __float_as_uint(r2);
+      int k1 = min(max((int)(bits >> kLogShift) - kLogBase, 0), kLogEntries);
+      float fr1 = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u) - 1.f;
+      int k2 = min(max((int)(bits >> kPcShift) - kPcBase, 0), kPcEntries);
+      float fr2 = __uint_as_float((bits & ((1u << kPcShift) - 1u)) | 0x3f800000u) - 1.f;
+      float2 c = tl[k1];
+      float4 d = tq[k2];
+      float f1 = fmaf(c.y, fr1, c.x), f2 = fmaf(d.y, fr2, d.x), f3 = fmaf(d.w, fr2, d.z);
       float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
       float q1x = Qxx * dx + Qxy * dy + Qxz * dz;
       float q2y = Qxy * dx + Qyy * dy + Qyz * dz;
@@ -665,14 +668,14 @@ template <bool kHardCut>
 __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
     const WalkBox *__restrict__ boxes, const uint32_t *__restrict__ gprefix, int nbox,
     uint32_t *__restrict__ gnext, uint32_t *__restrict__ stack_base, uint32_t *__restrict__ stats,
-    const float2 *__restrict__ g0, const float4 *__restrict__ g12, const float2 *__restrict__ glog, int entries,
-    float inv_delta, float rs2) {
+    const float2 *__restrict__ glog, const float4 *__restrict__ gpc, float rs2) {
   extern __shared__ float4 smem4[];
   float2 *tl = reinterpret_cast<float2 *>(smem4);
-  WarpLists *lists = reinterpret_cast<WarpLists *>(smem4 + kLogSmemF4);
+  float4 *tq = smem4 + kLogSmemF4;
+  WarpLists *lists = reinterpret_cast<WarpLists *>(smem4 + kLogSmemF4 + kPcEntries + 1);
   for (int i = threadIdx.x; i <= kLogEntries; i += kWalkThreads) tl[i] = glog[i];
+  for (int i = threadIdx.x; i <= kPcEntries; i += kWalkThreads) tq[i] = gpc[i];
   __syncthreads();
-  const float wmax = (float)(entries - 1);
   int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   WarpLists &wl = lists[wib];
   int64_t gwarp = (int64_t)blockIdx.x * kWalkWarps + wib;
@@ -819,7 +822,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
         npcl += cntv;
         __syncwarp();
         if (npcl >= 32) {
-          eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, g0, g12, inv_delta, wmax, npc);
+          eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, tl, tq, npc);
           npcl = 0;
         }
       }
@@ -853,7 +856,7 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
       if (lane == 0) atomicOr(wl.box.err, (uint32_t)kErrStackOverflow);
       continue;
     }
-    if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, g0, g12, inv_delta, wmax, npc);
+    if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, tl, tq, npc);
     if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, tl, npp);
     if (w.active) {
       // the tables are per unit LL: this box's 1/N^2
@@ -888,7 +891,7 @@ static int walk_grid(size_t smem) {
   // different tables stay launchable whatever order they were made in.
   static int cap_set = 0;
   if (!cap_set) {
-    size_t max_smem = sizeof(float4) * kLogSmemF4 + sizeof(WarpLists) * kWalkWarps;
+    size_t max_smem = sizeof(float4) * (kLogSmemF4 + kPcEntries + 1) + sizeof(WarpLists) * kWalkWarps;
     cudaFuncSetAttribute(k_tree_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     cudaFuncSetAttribute(k_tree_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     cap_set = 1;
@@ -932,16 +935,16 @@ WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &
 
 static void launch_walk(const WalkBox *boxes, const uint32_t *gprefix, int nbox, uint32_t *gnext, uint32_t *stack,
                         int64_t stack_words, uint32_t *stats, const LawTable &law, float rsphere, cudaStream_t st) {
-  size_t smem = sizeof(float4) * kLogSmemF4 + sizeof(WarpLists) * kWalkWarps;
+  size_t smem = sizeof(float4) * (kLogSmemF4 + kPcEntries + 1) + sizeof(WarpLists) * kWalkWarps;
   int grid = walk_grid(smem);
   int64_t max_grid = stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
   if (grid > max_grid) grid = (int)max_grid;
   if (law.hard_cut)
-    k_tree_walk<true><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
-                                                        law.tlog, law.entries, law.inv_delta, rsphere * rsphere);
+    k_tree_walk<true><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.tlog, law.tpc,
+                                                        rsphere * rsphere);
   else
-    k_tree_walk<false><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.t0, law.t12,
-                                                         law.tlog, law.entries, law.inv_delta, rsphere * rsphere);
+    k_tree_walk<false><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.tlog,
+                                                         law.tpc, rsphere * rsphere);
 }
 
 __global__ void k_set_walkbox(WalkBox *dst, WalkBox v) {
