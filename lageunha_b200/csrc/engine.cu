@@ -92,11 +92,13 @@ int tpm::check_params(const tpm_params *p) {
 }
 
 // ------------------------------------------------------------------ law table
-// Residual short-range law f(r)/N^2 and the table of OST/Model4TreeForce.c:
-// diff[i] = {-f/r, -(f'r - f)/(2 r^3), -(f''r^2 - 3f'r + 3f)/(2 r^5)} at
-// r = i*6/4096 with central differences of step 0.1*delta, entry 0 copied
-// from entry 1, slope[i] = (diff[i+1]-diff[i])/delta, last entry zero
-// (Model4TreeForce.c:48-91).
+// Residual short-range law f(r)/N^2 and its tables. OST/Model4TreeForce.c:
+// 48-91 tabulates {-f/r, -(f'r - f)/(2 r^3), -(f''r^2 - 3f'r + 3f)/(2 r^5)}
+// linearly at r = i*6/4096 (central differences of step 0.1*6/4096) and the
+// walk interpolates at r. The engine keeps the same three columns of the same
+// law but on grids uniform in log r^2 (indexed by the float bits of r^2, no
+// square root in the walk): -f/r on a fine grid (kLogMantissa bits per
+// octave), the two node columns on a coarse one (kPcMantissa bits).
 static const double kPmFit[8] = {1.0 / 256.0 / 256.0, 0.78224E+00, 0.37971E-06, -0.60338E+00,
                                  -0.34419E-07, -0.39741E+01, -0.10607E+01, -0.38145E+00};
 
@@ -120,95 +122,53 @@ static double law_f(int kind, double r, float eps, double rs, double LL) {
 
 static int build_law(tpm_ctx *c) {
   const tpm_params &p = c->prm;
-  if (c->law.t0 && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
+  if (c->law.tlog && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
       c->law_rs == p.rs_split && c->law_rsphere == p.rsphere)
     return 0;
-  const int NS = 4096;
-  const double range = 6.0;
-  float ran2nran = (float)(range / NS);
-  float invran = (float)(1.0 / ran2nran);
-  // the table is per unit LL (= N^2): the walk scales each box's forces by
+  // the tables are per unit LL (= N^2): the walk scales each box's forces by
   // its own 1/N^2, so boxes of every mesh size share one table
-  double LL = 1.0;
-  double dr = ran2nran * 0.1;
-  std::vector<double> diff((NS + 1) * 3, 0.0), slope(NS * 3, 0.0);
-  for (int i = 1; i < NS; i++) {
-    double r = (double)i * ran2nran;
-    double fp = (law_f(p.law, r + dr, p.epsilon, p.rs_split, LL) - law_f(p.law, r - dr, p.epsilon, p.rs_split, LL)) / (dr + dr);
-    double fpp = (law_f(p.law, r + 2 * dr, p.epsilon, p.rs_split, LL) - 2 * law_f(p.law, r, p.epsilon, p.rs_split, LL) +
-                  law_f(p.law, r - 2 * dr, p.epsilon, p.rs_split, LL)) / (4 * dr * dr);
-    double fr = law_f(p.law, r, p.epsilon, p.rs_split, LL);
-    diff[3 * i + 0] = -(fr / r);
-    diff[3 * i + 1] = -(0.5 * (fp * r - fr) / r / r / r);
-    diff[3 * i + 2] = -(0.5 * (fpp * r * r - 3 * fp * r + 3 * fr) / r / r / r / r / r);
-  }
-  for (int i = 0; i < NS; i++)
-    for (int k = 0; k < 3; k++) slope[3 * i + k] = (diff[3 * (i + 1) + k] - diff[3 * i + k]) / ran2nran;
-  for (int k = 0; k < 3; k++) {
-    slope[k] = slope[3 + k];
-    diff[k] = diff[3 + k];
-    diff[3 * (NS - 1) + k] = 0;
-    slope[3 * (NS - 1) + k] = 0;
-  }
-  int entries = (int)(p.rsphere * invran) + 2;
-  if (entries > NS) entries = NS;
-  std::vector<float2> t0(entries + 1);
-  std::vector<float4> t12(entries);
-  for (int i = 0; i < entries; i++) {
-    double dl = ran2nran;
-    t0[i] = make_float2((float)diff[3 * i], (float)(slope[3 * i] * dl));
-    t12[i] = make_float4((float)diff[3 * i + 1], (float)(slope[3 * i + 1] * dl), (float)diff[3 * i + 2],
-                         (float)(slope[3 * i + 2] * dl));
-  }
-  t0[entries] = make_float2(0.f, 0.f);
-  int hard_cut = 1;
-  if (p.law == TPM_LAW_GAUSSIAN) {
-    // the particle-particle column falls to zero at the first node kc at or
-    // beyond the cut: the pair term ramps to zero over the last interval
-    // (width 6/4096 cells) instead of stopping at r = rsphere exactly
-    int kc = (int)ceil((double)p.rsphere * invran);
-    if (kc >= 1 && kc < entries) {
-      for (int i = kc; i <= entries; i++) t0[i] = make_float2(0.f, 0.f);
-      t0[kc - 1].y = -t0[kc - 1].x;
-      hard_cut = 0;
-    }
-  }
-  // the particle-particle column on the log-spaced r^2 grid, from the same
-  // law (per unit LL), zero from the cut on
+  const double LL = 1.0;
+  // the reference's derivative step: a tenth of its table spacing 6/4096
+  const double dr = 0.1 * 6.0 / 4096.0;
+  const double rs2 = (double)p.rsphere * (double)p.rsphere;
+  // the reference law keeps its per-pair test r <= rsphere, so its column
+  // continues past the cut (the last bin before the cut interpolates the law
+  // itself); the Gaussian law's column is zero from the cut on, so the pair
+  // term ramps to zero over the last bin and the walk needs no pair test
+  const int hard_cut = p.law == TPM_LAW_GAUSSIAN ? 0 : 1;
+  auto at_bits = [](uint32_t bits) {
+    float sf;
+    memcpy(&sf, &bits, 4);
+    return (double)sf;
+  };
+  // the particle-particle column -f/r on the log-spaced r^2 grid
   std::vector<float2> tlog(kLogEntries + 1);
   {
     std::vector<double> v(kLogEntries + 1);
-    double rs2 = (double)p.rsphere * (double)p.rsphere;
     for (int k = 0; k <= kLogEntries; k++) {
-      uint32_t bits = (uint32_t)(kLogBase + k) << kLogShift;
-      float sf;
-      memcpy(&sf, &bits, 4);
-      double s = (double)sf, r = sqrt(s);
-      v[k] = s >= rs2 ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
+      double s = at_bits((uint32_t)(kLogBase + k) << kLogShift), r = sqrt(s);
+      v[k] = (s >= rs2 && !hard_cut) ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
     }
     for (int k = 0; k < kLogEntries; k++)
       tlog[k] = make_float2((float)v[k], (float)((v[k + 1] - v[k]) * (double)(1 << kLogMantissa)));
     tlog[kLogEntries] = make_float2(0.f, 0.f);
   }
-  // the node terms' derivative columns on the coarse log grid, with the same
-  // central differences as the linear table
+  // the node terms' derivative columns (Model4TreeForce.c:48-91:
+  // -(f'r - f)/(2 r^3) and -(f''r^2 - 3f'r + 3f)/(2 r^5), central
+  // differences) on the coarse log grid; the node test r <= rsphere is always
+  // made, so the columns continue past the cut
   std::vector<float4> tpc(kPcEntries + 1);
   {
     std::vector<double> f2(kPcEntries + 1), f3(kPcEntries + 1);
-    double rs2 = (double)p.rsphere * (double)p.rsphere;
     for (int k = 0; k <= kPcEntries; k++) {
-      uint32_t bits = (uint32_t)(kPcBase + k) << kPcShift;
-      float sf;
-      memcpy(&sf, &bits, 4);
-      double s = (double)sf, r = sqrt(s);
-      if (s >= rs2) {
-        f2[k] = f3[k] = 0.0;
-        continue;
-      }
-      double fp = (law_f(p.law, r + dr, p.epsilon, p.rs_split, LL) - law_f(p.law, r - dr, p.epsilon, p.rs_split, LL)) / (dr + dr);
-      double fpp = (law_f(p.law, r + 2 * dr, p.epsilon, p.rs_split, LL) - 2 * law_f(p.law, r, p.epsilon, p.rs_split, LL) +
-                    law_f(p.law, r - 2 * dr, p.epsilon, p.rs_split, LL)) / (4 * dr * dr);
+      double s = at_bits((uint32_t)(kPcBase + k) << kPcShift), r = sqrt(s);
+      double fm2 = law_f(p.law, r - 2 * dr, p.epsilon, p.rs_split, LL);
+      double fm1 = law_f(p.law, r - dr, p.epsilon, p.rs_split, LL);
       double fr = law_f(p.law, r, p.epsilon, p.rs_split, LL);
+      double fp1 = law_f(p.law, r + dr, p.epsilon, p.rs_split, LL);
+      double fp2 = law_f(p.law, r + 2 * dr, p.epsilon, p.rs_split, LL);
+      double fp = (fp1 - fm1) / (dr + dr);
+      double fpp = (fp2 - 2 * fr + fm2) / (4 * dr * dr);
       f2[k] = -(0.5 * (fp * r - fr) / r / r / r);
       f3[k] = -(0.5 * (fpp * r * r - 3 * fp * r + 3 * fr) / r / r / r / r / r);
     }
@@ -218,27 +178,16 @@ static int build_law(tpm_ctx *c) {
                            (float)((f3[k + 1] - f3[k]) * sc));
     tpc[kPcEntries] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  if (c->law.t0 || c->law.t12) CK(cudaStreamSynchronize(c->st));
+  if (c->law.tlog || c->law.tpc) CK(cudaStreamSynchronize(c->st));
   if (c->law.tlog) cudaFree(c->law.tlog);
   if (c->law.tpc) cudaFree(c->law.tpc);
   c->law.tlog = nullptr;
   c->law.tpc = nullptr;
-  if (c->law.t0) cudaFree(c->law.t0);
-  if (c->law.t12) cudaFree(c->law.t12);
-  c->law.t0 = nullptr;
-  c->law.t12 = nullptr;
-  CK(cudaMalloc(&c->law.t0, sizeof(float2) * (entries + 1)));
-  CK(cudaMalloc(&c->law.t12, sizeof(float4) * entries));
-  CK(cudaMemcpy(c->law.t0, t0.data(), sizeof(float2) * (entries + 1), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->law.t12, t12.data(), sizeof(float4) * entries, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c->law.tlog, sizeof(float2) * (kLogEntries + 1)));
   CK(cudaMemcpy(c->law.tlog, tlog.data(), sizeof(float2) * (kLogEntries + 1), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c->law.tpc, sizeof(float4) * (kPcEntries + 1)));
   CK(cudaMemcpy(c->law.tpc, tpc.data(), sizeof(float4) * (kPcEntries + 1), cudaMemcpyHostToDevice));
-  c->law.entries = entries;
   c->law.hard_cut = hard_cut;
-  c->law.delta = ran2nran;
-  c->law.inv_delta = invran;
   c->law_n = p.n_mesh;
   c->law_eps = p.epsilon;
   c->law_kind = p.law;
@@ -524,7 +473,7 @@ WalkBox tpm::ctx_walk_box(const tpm_ctx *c) {
   tp.rsphere = c->prm.rsphere;
   tp.cell_per_unit = (float)((double)c->g.n / 4294967296.0);
   tp.mass = c->prm.particle_mass;
-  return walk_box(tp, c->spos, c->tb, c->law, c->ftree, c->err);
+  return walk_box(tp, c->spos, c->tb, c->ftree, c->err);
 }
 
 int64_t tpm::ctx_bytes(int n_mesh, int64_t np) {
@@ -627,8 +576,6 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->st) cudaStreamSynchronize(c->st);
   free_particles(c);
   free_mesh(c);
-  if (c->law.t0) cudaFree(c->law.t0);
-  if (c->law.t12) cudaFree(c->law.t12);
   if (c->law.tlog) cudaFree(c->law.tlog);
   if (c->law.tpc) cudaFree(c->law.tpc);
   if (c->err) cudaFree(c->err);

@@ -100,7 +100,7 @@ struct WalkBox {
   const uint32_t *ngroups;  // device word: the box's group count
   float *ftree;
   uint32_t *err;
-  float cpu, cpi, mass, inv_ll;
+  float cpu, mass, inv_ll;
 };
 struct TreeBuffers {
   int64_t cap_nodes = 0;
@@ -161,18 +161,14 @@ constexpr int kPcShift = 23 - kPcMantissa;
 constexpr int kPcBase = (127 - 8) << kPcMantissa;
 constexpr int kPcEntries = 14 << kPcMantissa;
 struct LawTable {
-  float2 *t0 = nullptr;
-  float4 *t12 = nullptr;
-  float2 *tlog = nullptr;  // [kLogEntries + 1]
-  float4 *tpc = nullptr;   // [kPcEntries + 1]
-  int entries = 0;
-  float delta = 0, inv_delta = 0;
+  float2 *tlog = nullptr;  // [kLogEntries + 1] {-f/r, slope per bin}
+  float4 *tpc = nullptr;   // [kPcEntries + 1] the two node columns and slopes
   // 1: the walk tests r <= rsphere per pair (the reference's cut);
-  // 0: t0 is zero from the cut on, so the pair test is not needed
+  // 0: tlog is zero from the cut on, so the pair test is not needed
   int hard_cut = 1;
 };
-WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, const LawTable &law,
-                 float *ftree, uint32_t *err);
+WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, float *ftree,
+                 uint32_t *err);
 // One launch over the groups of every box (boxes: device array); the boxes
 // share law (same kind, softening, split and cut) and rsphere.
 void tree_walk_multi(const WalkBox *boxes, int nbox, uint32_t *gprefix, uint32_t *gnext, uint32_t *stack,

@@ -479,25 +479,6 @@ struct WalkCtx {
   uint32_t rx, ry, rz;    // u_ref
 };
 
-// Hardware reciprocal square root (MUFU), flushing denormals: the walk's
-// separations are at least 2^-32 cells apart or exactly zero.
-TPM_D float rsqrt_approx(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// Linear-table lookup at w = r/delta (w >= 0) without float<->int
-// conversions: adding 1.5*2^23 rounding toward -inf leaves floor(w) in the
-// low mantissa.
-TPM_D int table_index(float w, float &frac) {
-  const float magic = 12582912.0f;
-  float v = __fadd_rd(w, magic);
-  float fl = v - magic;
-  frac = w - fl;
-  return __float_as_int(v) - 0x4B400000;
-}
-
 // One source against this lane's target: the reference's AddPar
 // (OST/ost.ver2.c:279-293) without the mass factor. The law comes from the
 // table indexed by the float bits of r^2 (cells^2): the exponent and the top
@@ -913,8 +894,8 @@ int64_t walk_stack_words() {
   return (int64_t)sms * 2 * kWalkWarps * (kStackCap - kStackSmem);
 }
 
-WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, const LawTable &law,
-                 float *ftree, uint32_t *err) {
+WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, float *ftree,
+                 uint32_t *err) {
   WalkBox b;
   b.spos = spos;
   b.walkA = tb.walkA;
@@ -927,7 +908,6 @@ WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &
   b.ftree = ftree;
   b.err = err;
   b.cpu = tp.cell_per_unit;
-  b.cpi = tp.cell_per_unit * law.inv_delta;
   b.mass = tp.mass;
   b.inv_ll = (float)(1.0 / ((double)tp.n * (double)tp.n));
   return b;
@@ -955,7 +935,7 @@ void tree_walk(const TreeParams &tp, const uint32_t *spos, int64_t np, const Tre
                const LawTable &law, float *ftree, uint32_t *err, cudaStream_t st, int64_t *launches) {
   (void)np;
   // the box record goes to the device with the launch that precedes the walk
-  k_set_walkbox<<<1, 32, 0, st>>>(tb.walkbox, walk_box(tp, spos, tb, law, ftree, err));
+  k_set_walkbox<<<1, 32, 0, st>>>(tb.walkbox, walk_box(tp, spos, tb, ftree, err));
   // tb.counters[1] is the next-group counter (zeroed before tree_groups)
   launch_walk(tb.walkbox, nullptr, 1, &tb.counters[1], tb.stack, tb.stack_words, tb.counters, law, tp.rsphere, st);
   if (launches) *launches += 2;
