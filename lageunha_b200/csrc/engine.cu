@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -141,22 +142,29 @@ static int build_law(tpm_ctx *c) {
     memcpy(&sf, &bits, 4);
     return (double)sf;
   };
-  // the particle-particle column -f/r on the log-spaced r^2 grid
+  // the particle-particle column -f/r on the log-spaced grid of
+  // s = r^2 + kLogR2Floor, held at its value at r = 2^-10 cells below that
+  // (the reference's table is flat below its first entry, r = 6/4096, and
+  // its fitted long-range law does not vanish at r = 0)
   std::vector<float2> tlog(kLogEntries + 1);
   {
     std::vector<double> v(kLogEntries + 1);
     for (int k = 0; k <= kLogEntries; k++) {
-      double s = at_bits((uint32_t)(kLogBase + k) << kLogShift), r = sqrt(s);
-      v[k] = (s >= rs2 && !hard_cut) ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
+      double s = at_bits((uint32_t)(kLogBase + k) << kLogShift);
+      double r2 = s - (double)kLogR2Floor, r = std::max(sqrt(std::max(r2, 0.0)), 0.0009765625);
+      v[k] = (r2 >= rs2 && !hard_cut) ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
     }
-    for (int k = 0; k < kLogEntries; k++)
-      tlog[k] = make_float2((float)v[k], (float)((v[k + 1] - v[k]) * (double)(1 << kLogMantissa)));
+    const double sc = (double)(1 << kLogMantissa);
+    for (int k = 0; k < kLogEntries; k++) {
+      double d = (v[k + 1] - v[k]) * sc;
+      tlog[k] = make_float2((float)(v[k] - d), (float)d);
+    }
     tlog[kLogEntries] = make_float2(0.f, 0.f);
   }
   // the node terms' derivative columns (Model4TreeForce.c:48-91:
   // -(f'r - f)/(2 r^3) and -(f''r^2 - 3f'r + 3f)/(2 r^5), central
-  // differences) on the coarse log grid; the node test r <= rsphere is always
-  // made, so the columns continue past the cut
+  // differences) on the coarse log grid of r^2; the node test r <= rsphere is
+  // always made, so the columns continue past the cut
   std::vector<float4> tpc(kPcEntries + 1);
   {
     std::vector<double> f2(kPcEntries + 1), f3(kPcEntries + 1);
@@ -173,9 +181,10 @@ static int build_law(tpm_ctx *c) {
       f3[k] = -(0.5 * (fpp * r * r - 3 * fp * r + 3 * fr) / r / r / r / r / r);
     }
     const double sc = (double)(1 << kPcMantissa);
-    for (int k = 0; k < kPcEntries; k++)
-      tpc[k] = make_float4((float)f2[k], (float)((f2[k + 1] - f2[k]) * sc), (float)f3[k],
-                           (float)((f3[k + 1] - f3[k]) * sc));
+    for (int k = 0; k < kPcEntries; k++) {
+      double d2 = (f2[k + 1] - f2[k]) * sc, d3 = (f3[k + 1] - f3[k]) * sc;
+      tpc[k] = make_float4((float)(f2[k] - d2), (float)d2, (float)(f3[k] - d3), (float)d3);
+    }
     tpc[kPcEntries] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   if (c->law.tlog || c->law.tpc) CK(cudaStreamSynchronize(c->st));

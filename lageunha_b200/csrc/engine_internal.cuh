@@ -141,21 +141,23 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
 void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
                  uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
                  int64_t *launches);
-// Short-range law table in index units: at w = r / delta, entry n = floor(w)
-// and frac = w - n, column c is diff_c[n] + slope_c[n]*delta*frac
-// (OST/Model4TreeForce.c:34-46). t0 = {diff0, slope0*delta},
-// t12 = {diff1, slope1*delta, diff2, slope2*delta}.
-// The particle-particle column once more, indexed by the float bits of r^2:
-// entry k covers r^2 in [s_k, s_{k+1}) with s_k the float whose top bits are
-// (kLogBase + k) << kLogShift, i.e. 2^kLogMantissa bins per octave of r^2 from
-// 2^-20 to 2^6 cells^2; {value at s_k, (value at s_{k+1} - value) * 2^kLogMantissa}.
+// The short-range law's columns on grids uniform in log r^2, indexed by the
+// float bits of s = r^2 + kLogR2Floor (cells^2). Entry k covers
+// [s_k, s_{k+1}), s_k the float whose top bits are (kLogBase + k) <<
+// kLogShift: 2^kLogMantissa bins per octave from 2^-20 (= kLogR2Floor, so
+// every s lands in the table without a lower clamp) to 2^6 cells^2. With m
+// the float of s's in-bin mantissa bits under exponent 0 (m in [1, 1 +
+// 2^-kLogMantissa)), the column is c.x + c.y * m: c.y = (v_{k+1} - v_k) *
+// 2^kLogMantissa and c.x = v_k - c.y, v_k the value at r^2 = s_k - kLogR2Floor.
+constexpr float kLogR2Floor = 9.5367431640625e-07f;  // 2^-20
 constexpr int kLogMantissa = 7;
 constexpr int kLogShift = 23 - kLogMantissa;
 constexpr int kLogBase = (127 - 20) << kLogMantissa;
 constexpr int kLogEntries = 26 << kLogMantissa;
-// The node terms' derivative columns (f2, f3 of the linear table t12) on a
-// coarser log grid of r^2, 2^kPcMantissa bins per octave from 2^-8 to 2^6
-// cells^2 (accepted nodes are never closer): {f2, df2 * 2^m, f3, df3 * 2^m}.
+// The node terms' derivative columns f2, f3 on a coarser log grid of r^2,
+// 2^kPcMantissa bins per octave from 2^-8 to 2^6 cells^2 (closer nodes take
+// the first bin), in the same c.x + c.y * m form: {f2 - df2, df2, f3 - df3,
+// df3} with df = (f_{k+1} - f_k) * 2^kPcMantissa.
 constexpr int kPcMantissa = 5;
 constexpr int kPcShift = 23 - kPcMantissa;
 constexpr int kPcBase = (127 - 8) << kPcMantissa;

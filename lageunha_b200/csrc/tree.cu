@@ -481,22 +481,24 @@ struct WalkCtx {
 
 // One source against this lane's target: the reference's AddPar
 // (OST/ost.ver2.c:279-293) without the mass factor. The law comes from the
-// table indexed by the float bits of r^2 (cells^2): the exponent and the top
-// kLogMantissa mantissa bits pick the bin, the remaining mantissa bits are the
-// position inside it, so neither a square root nor a conversion is needed.
-// r2 = 0 (the target itself) lands in bin 0 with a zero separation, adding
-// nothing. kHardCut: the per-pair r^2 <= rsphere^2 test of the reference law;
-// the table is zero from the cut on, which is all the Gaussian law needs.
+// table indexed by the float bits of s = r^2 + kLogR2Floor (cells^2): the
+// exponent and the top kLogMantissa mantissa bits pick the bin, the remaining
+// mantissa bits are the position inside it, so neither a square root nor a
+// conversion is needed, and s >= 2^-20 needs no lower clamp. The target
+// itself (r = 0) lands in bin 0 with a zero separation, adding nothing.
+// kHardCut: the per-pair cut of the reference law, tested as s <= rsphere^2
+// (a cut 2^-20 cells^2 inside r^2 <= rsphere^2); the Gaussian law's table is
+// zero from the cut on and needs no test.
 template <bool kHardCut>
 TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, const float2 *__restrict__ tl, float &ax,
                    float &ay, float &az) {
   float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
-  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
   uint32_t bits = __float_as_uint(r2);
-  int k = min(max((int)(bits >> kLogShift) - kLogBase, 0), kLogEntries);
-  float frac = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u) - 1.f;
+  int k = min((int)(bits >> kLogShift) - kLogBase, kLogEntries);
+  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
   float2 c = tl[k];
-  float f = fmaf(c.y, frac, c.x);
+  float f = fmaf(c.y, m, c.x);
   if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
   ay = fmaf(dy, f, ay);
@@ -573,8 +575,8 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 }
 
 // Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
-// and z components on their own axes. Coordinates are in cells; the linear
-// tables (t0, t12, index w = r / delta) give the law and its derivatives.
+// and z components on their own axes. Coordinates are in cells; the log-r^2
+// tables in shared memory give the law and its derivatives.
 TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpu, float rs2,
                    const float2 *__restrict__ tl, const float4 *__restrict__ tq, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
@@ -594,17 +596,17 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, floa
     for (int j = 0; j < m; j++) {
       float4 c0 = wl.stage[3 * j], q1 = wl.stage[3 * j + 1], q2 = wl.stage[3 * j + 2];
       float dx = w.tx - c0.x, dy = w.ty - c0.y, dz = w.tz - c0.z;
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
       // f1 from the particle-particle table, f2 and f3 from the coarse one,
       // both indexed by the bits of r^2 (shared memory)
       uint32_t bits = __float_as_uint(r2);
-      int k1 = min(max((int)(bits >> kLogShift) - kLogBase, 0), kLogEntries);
-      float fr1 = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u) - 1.f;
+      int k1 = min((int)(bits >> kLogShift) - kLogBase, kLogEntries);
+      float m1 = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
       int k2 = min(max((int)(bits >> kPcShift) - kPcBase, 0), kPcEntries);
-      float fr2 = __uint_as_float((bits & ((1u << kPcShift) - 1u)) | 0x3f800000u) - 1.f;
+      float m2 = __uint_as_float((bits & ((1u << kPcShift) - 1u)) | 0x3f800000u);
       float2 c = tl[k1];
       float4 d = tq[k2];
-      float f1 = fmaf(c.y, fr1, c.x), f2 = fmaf(d.y, fr2, d.x), f3 = fmaf(d.w, fr2, d.z);
+      float f1 = fmaf(c.y, m1, c.x), f2 = fmaf(d.y, m2, d.x), f3 = fmaf(d.w, m2, d.z);
       float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
       float q1x = Qxx * dx + Qxy * dy + Qxz * dz;
       float q2y = Qxy * dx + Qyy * dy + Qyz * dz;
