@@ -26,9 +26,9 @@
 
 namespace tpm {
 
-constexpr int kBuildTile = 1024;
 constexpr int kBuildThreads = 256;
-constexpr int kBuildGrid = 148 * 4;
+constexpr int kBuildGrid = 148 * 8;
+constexpr int kScanGrid = 148 * 2;
 
 TPM_D float wrapf(uint32_t a, uint32_t b, float cpu) { return (float)(int32_t)(a - b) * cpu; }
 
@@ -64,51 +64,105 @@ __global__ void k_tree_root(int64_t np, TreeBuffers tb, uint32_t n, int sub_bits
   }
 }
 
+// The level kernels give each node a segment of 8 lanes, lane d owning the
+// node's d-th octant (its level-(l+1) digit): the eight child boundaries are
+// found by eight independent binary searches instead of one chain of seven,
+// and the children are written in parallel. Items are (node, digit) pairs;
+// the loops over them are warp-uniform, so the segment shuffles stay
+// converged.
+constexpr int kScanChunk = 4096;  // nodes per block of the per-level scan
+
+struct ChildRange {
+  uint32_t node;  // absolute index of the segment's node
+  bool valid;     // the node exists (item < 8 * nodes of the level)
+  uint32_t lo, hi;  // this lane's child [lo, hi), empty when the node does not split
+};
+
+TPM_D ChildRange child_range(const uint64_t *__restrict__ key, const TreeBuffers &tb, uint32_t b,
+                             uint32_t nn, uint64_t item, int l, int shift) {
+  int d = threadIdx.x & 7;
+  ChildRange r;
+  r.valid = item < (uint64_t)nn * 8u;
+  r.node = b + (uint32_t)(item >> 3);
+  uint32_t s = 0, c = 0;
+  if (r.valid) {
+    s = tb.start[r.node];
+    c = tb.count[r.node];
+  }
+  bool split = r.valid && c >= (uint32_t)kLeafMin && l < kAxisBits;
+  uint32_t bnd = s;
+  if (split && d > 0) bnd = lower_digit(key, s, s + c, shift, (uint32_t)d);
+  uint32_t nxt = __shfl_down_sync(0xffffffffu, bnd, 1, 8);
+  if (d == 7) nxt = s + c;
+  r.lo = bnd;
+  r.hi = split ? nxt : bnd;
+  return r;
+}
+
 // Count the non-empty children of every level-l node that splits.
 __global__ void __launch_bounds__(kBuildThreads) k_tree_count(const uint64_t *__restrict__ key,
                                                               TreeBuffers tb, int l) {
   uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
   uint32_t nn = e - b;
-  uint32_t ntiles = (nn + kBuildTile - 1) / kBuildTile;
-  __shared__ uint32_t red[kBuildThreads / 32];
+  int lane = threadIdx.x & 31;
   int shift = 3 * (kAxisBits - 1 - l);
-  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    uint32_t local = 0;
-    for (int r = 0; r < kBuildTile / kBuildThreads; r++) {
-      uint32_t i = t * kBuildTile + r * kBuildThreads + threadIdx.x;
-      if (i < nn) {
-        uint32_t node = b + i;
-        uint32_t s = tb.start[node], c = tb.count[node];
-        uint32_t nch = 0;
-        if (c >= (uint32_t)kLeafMin && l < kAxisBits) {
-          uint32_t lo = s, hi = s + c;
-          uint32_t prev = lo;
-          for (uint32_t d = 1; d <= 8; d++) {
-            uint32_t bnd = d < 8 ? lower_digit(key, prev, hi, shift, d) : hi;
-            if (bnd > prev) nch++;
-            prev = bnd;
-          }
-        }
-        tb.nchild[node] = nch;
-        local += nch;
-      }
+  const unsigned seg = 0xffu << (lane & ~7);
+  uint64_t total = (uint64_t)nn * 8u, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    ChildRange cr = child_range(key, tb, b, nn, base + lane, l, shift);
+    unsigned m = __ballot_sync(0xffffffffu, cr.hi > cr.lo) & seg;
+    if (cr.valid && (lane & 7) == 0) tb.nchild[cr.node] = (uint32_t)__popc(m);
+  }
+}
+
+// Per-level exclusive scan of nchild over chunks of kScanChunk nodes: the
+// prefix within the chunk goes to child[node] (the write pass adds the
+// chunk's offset and overwrites it), the chunk's total to tile_sum[chunk].
+__global__ void __launch_bounds__(1024) k_tree_scan_chunks(TreeBuffers tb, int l) {
+  __shared__ uint32_t wsum[32];
+  uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
+  uint32_t nn = e - b;
+  uint32_t nchunks = (nn + kScanChunk - 1) / kScanChunk;
+  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (uint32_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    uint32_t base = ch * kScanChunk;
+    uint32_t v[4], s = 0;
+    for (int j = 0; j < 4; j++) {
+      uint32_t i = base + 4 * tid + j;
+      v[j] = i < nn ? tb.nchild[b + i] : 0u;
+      s += v[j];
     }
-    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+    uint32_t x = s;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t s = 0;
-      for (int w = 0; w < kBuildThreads / 32; w++) s += red[w];
-      tb.tile_sum[t] = s;
+    if (warp == 0) {
+      uint32_t t = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      wsum[lane] = t;
     }
+    __syncthreads();
+    uint32_t run = (warp ? wsum[warp - 1] : 0u) + x - s;
+    for (int j = 0; j < 4; j++) {
+      uint32_t i = base + 4 * tid + j;
+      if (i < nn) tb.child[b + i] = run;
+      run += v[j];
+    }
+    if (tid == 0) tb.tile_sum[ch] = wsum[31];
     __syncthreads();
   }
 }
 
-// Exclusive scan of the tile sums of level l and the extent of level l+1.
+// Exclusive scan of the chunk sums of level l and the extent of level l+1.
 __global__ void __launch_bounds__(1024) k_tree_scan(TreeBuffers tb, int l, uint32_t *err) {
   uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
-  uint32_t ntiles = (e - b + kBuildTile - 1) / kBuildTile;
+  uint32_t ntiles = (e - b + kScanChunk - 1) / kScanChunk;
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t carry;
   int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -142,15 +196,27 @@ __global__ void __launch_bounds__(1024) k_tree_scan(TreeBuffers tb, int l, uint3
     uint64_t end = (uint64_t)e + carry;
     if (end > (uint64_t)tb.cap_nodes) {
       atomicOr(err, (uint32_t)kErrNodeOverflow);
-      end = e;  // stop refining
-      // leave the level's nodes as leaves
+      end = e;  // stop refining: the level's nodes stay leaves
     }
     tb.level_range[2 * (l + 1)] = e;
     tb.level_range[2 * (l + 1) + 1] = (uint32_t)end;
   }
 }
 
-// Write the children of level-l nodes.
+// The three axis coordinates interleaved in a Morton key (bit 3i + a of the
+// key is bit i of axis a).
+TPM_D uint32_t morton_compact(uint64_t x) {
+  x &= 0x1249249249249249ull;
+  x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+  x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+  x = (x ^ (x >> 8)) & 0x1f0000ff0000ffull;
+  x = (x ^ (x >> 16)) & 0x1f00000000ffffull;
+  x = (x ^ (x >> 32)) & 0x1fffffull;
+  return (uint32_t)x;
+}
+
+// Write the children of level-l nodes: node records of level l+1 in the
+// order of their parents, siblings contiguous in octant order.
 __global__ void __launch_bounds__(kBuildThreads) k_tree_write(const uint64_t *__restrict__ key,
                                                               TreeBuffers tb, int l, uint32_t n,
                                                               int sub_bits) {
@@ -158,78 +224,44 @@ __global__ void __launch_bounds__(kBuildThreads) k_tree_write(const uint64_t *__
   uint32_t e1 = tb.level_range[2 * (l + 1) + 1];
   bool overflow = (e1 == e);  // capacity hit: nothing written below this level
   uint32_t nn = e - b;
-  uint32_t ntiles = (nn + kBuildTile - 1) / kBuildTile;
-  __shared__ uint32_t wsum[kBuildThreads / 32];
-  __shared__ uint32_t carry;
-  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int lane = threadIdx.x & 31;
   int shift = 3 * (kAxisBits - 1 - l);
+  const unsigned seg = 0xffu << (lane & ~7);
   int child_level = l + 1;
   // child cube: side 2^(13-child_level) q units
   uint32_t cside_q = 1u << (kAxisBits - child_level);
   float half_cells = (float)((double)cside_q * 0.5 / (double)(1u << sub_bits));
-  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (tid == 0) carry = tb.tile_sum[t];
-    __syncthreads();
-    for (int r = 0; r < kBuildTile / kBuildThreads; r++) {
-      uint32_t i = t * kBuildTile + r * kBuildThreads + tid;
-      uint32_t node = b + i;
-      uint32_t nch = (i < nn) ? tb.nchild[node] : 0u;
-      if (overflow && i < nn) {
-        nch = 0;
-        tb.nchild[node] = 0;
+  uint64_t total = (uint64_t)nn * 8u, stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    ChildRange cr = child_range(key, tb, b, nn, base + lane, l, shift);
+    bool ne = !overflow && cr.hi > cr.lo;
+    uint32_t first = 0;
+    if (cr.valid) first = e + tb.child[cr.node] + tb.tile_sum[(cr.node - b) / kScanChunk];
+    // every lane has read child[node] before the segment's lane 0 rewrites it
+    unsigned m = __ballot_sync(0xffffffffu, ne) & seg;
+    if (ne) {
+      uint32_t slot = first + (uint32_t)__popc(m & ((1u << lane) - 1u));
+      tb.start[slot] = cr.lo;
+      tb.count[slot] = cr.hi - cr.lo;
+      tb.child[slot] = 0;
+      tb.nchild[slot] = 0;
+      tb.level[slot] = (uint8_t)child_level;
+      // cube of the child from its first key
+      uint64_t k = key[cr.lo];
+      uint32_t q[3] = {morton_compact(k), morton_compact(k >> 1), morton_compact(k >> 2)};
+      uint32_t cu[3];
+      for (int a = 0; a < 3; a++) {
+        uint32_t qc = q[a] & ~(cside_q - 1u);
+        double cells = ((double)qc + 0.5 * (double)cside_q) / (double)(1u << sub_bits);
+        double fr = cells / (double)n;
+        fr -= floor(fr);
+        cu[a] = (uint32_t)(unsigned long long)llrint(fr * 4294967296.0);
       }
-      uint32_t x = nch;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      if (lane == 31) wsum[warp] = x;
-      __syncthreads();
-      uint32_t pre = carry;
-      for (int w = 0; w < warp; w++) pre += wsum[w];
-      pre += x - nch;
-      if (i < nn && nch > 0) {
-        uint32_t first = e + pre;
-        tb.child[node] = first;
-        uint32_t s = tb.start[node], c = tb.count[node];
-        uint32_t hi = s + c, prev = s, slot = first;
-        for (uint32_t d = 1; d <= 8; d++) {
-          uint32_t bnd = d < 8 ? lower_digit(key, prev, hi, shift, d) : hi;
-          if (bnd > prev) {
-            tb.start[slot] = prev;
-            tb.count[slot] = bnd - prev;
-            tb.child[slot] = 0;
-            tb.nchild[slot] = 0;
-            tb.level[slot] = (uint8_t)child_level;
-            // cube of the child from its first key
-            uint64_t k = key[prev];
-            uint32_t q[3] = {0, 0, 0};
-            for (int bit = 0; bit < kAxisBits; bit++) {
-              q[0] |= (uint32_t)((k >> (3 * bit)) & 1u) << bit;
-              q[1] |= (uint32_t)((k >> (3 * bit + 1)) & 1u) << bit;
-              q[2] |= (uint32_t)((k >> (3 * bit + 2)) & 1u) << bit;
-            }
-            uint32_t cu[3];
-            for (int a = 0; a < 3; a++) {
-              uint32_t qc = q[a] & ~(cside_q - 1u);
-              double cells = ((double)qc + 0.5 * (double)cside_q) / (double)(1u << sub_bits);
-              double fr = cells / (double)n;
-              fr -= floor(fr);
-              cu[a] = (uint32_t)(unsigned long long)llrint(fr * 4294967296.0);
-            }
-            tb.geo[slot] = make_uint4(cu[0], cu[1], cu[2], __float_as_uint(half_cells));
-            slot++;
-          }
-          prev = bnd;
-        }
-      }
-      __syncthreads();
-      if (tid == 0) {
-        uint32_t s = 0;
-        for (int w = 0; w < kBuildThreads / 32; w++) s += wsum[w];
-        carry += s;
-      }
-      __syncthreads();
+      tb.geo[slot] = make_uint4(cu[0], cu[1], cu[2], __float_as_uint(half_cells));
+    }
+    if (cr.valid && (lane & 7) == 0) {
+      tb.child[cr.node] = m ? first : 0u;
+      if (overflow) tb.nchild[cr.node] = 0;
     }
   }
 }
@@ -327,9 +359,10 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
   int64_t nl = 1;
   for (int l = 0; l < kAxisBits; l++) {
     k_tree_count<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l);
+    k_tree_scan_chunks<<<kScanGrid, 1024, 0, st>>>(tb, l);
     k_tree_scan<<<1, 1024, 0, st>>>(tb, l, err);
     k_tree_write<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l, tp.n, tp.sub_bits);
-    nl += 3;
+    nl += 4;
   }
   float inv_theta2 = 1.f / tp.theta2;
   for (int l = kAxisBits; l >= 0; l--) {
@@ -456,6 +489,7 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 
 // ------------------------------------------------------------------ walk
 constexpr int kWalkWarps = 16;
+constexpr int kWalkBlocksPerSm = 2;  // resident CTAs per SM the registers are budgeted for
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kStackSmem = 640;    // per-warp stack entries in shared memory
 constexpr int kStackCap = 8192;    // entries beyond kStackSmem live in global memory
@@ -648,7 +682,7 @@ struct WarpStack {
 // gprefix[b] <= g < gprefix[b+1]). The boxes share the law table, which is
 // per unit LL: each box's forces are scaled by its 1/N^2 at the end.
 template <bool kHardCut>
-__global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
+__global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
     const WalkBox *__restrict__ boxes, const uint32_t *__restrict__ gprefix, int nbox,
     uint32_t *__restrict__ gnext, uint32_t *__restrict__ stack_base, uint32_t *__restrict__ stats,
     const float2 *__restrict__ glog, const float4 *__restrict__ gpc, float rs2) {
@@ -869,9 +903,8 @@ __global__ void __launch_bounds__(kWalkThreads, 2) k_tree_walk(
 }
 
 static int walk_grid(size_t smem) {
-  // The dynamic shared-memory cap is raised once to the largest table a law
-  // can have (4096 + 1 entries), so graphs captured for contexts with
-  // different tables stay launchable whatever order they were made in.
+  // The dynamic shared-memory cap is raised once (the tables and the warp
+  // records have fixed sizes, the same for every law and context).
   static int cap_set = 0;
   if (!cap_set) {
     size_t max_smem = sizeof(float4) * (kLogSmemF4 + kPcEntries + 1) + sizeof(WarpLists) * kWalkWarps;
@@ -893,7 +926,7 @@ int64_t walk_stack_words() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int64_t)sms * 2 * kWalkWarps * (kStackCap - kStackSmem);
+  return (int64_t)sms * kWalkBlocksPerSm * kWalkWarps * (kStackCap - kStackSmem);
 }
 
 WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, float *ftree,
