@@ -74,8 +74,13 @@ TPM_D void tsc_w(float xmin, float &w1, float &w2, float &w3, int &sign) {
   w2 = w3 + d;
 }
 
-constexpr int kDepNx = 16;            // x extent of the deposit tile: [t-4, t+12)
-constexpr int kDepNy = kTile + 3;     // y/z extent: [t-1, t+9]
+// The deposit tile's accumulator covers nodes [t-1, t+11) per axis (the
+// stencils of particles in [t, t+8) reach [t-1, t+9]) with strides 1, 12,
+// 144: a 4x4x2 block of home nodes, which 32 Morton-consecutive particles at
+// one per cell occupy, falls on 32 distinct shared-memory banks, as do its 27
+// shifted copies.
+constexpr int kDepNx = 12;
+constexpr int kDepNy = 12;
 constexpr int kDepCells = kDepNx * kDepNy * kDepNy;
 constexpr int kDepThreads = 256;
 
@@ -146,27 +151,37 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
   }
 }
 
-// Adds a tile's shared-memory accumulator to the periodic mesh.
+// Adds a tile's shared-memory accumulator (origin ox = t-1 per axis) to the
+// periodic mesh. vec4: the mesh's x rows are added as float4 groups aligned
+// to 4 cells, [t-4, t), ..., [t+8, t+12), read from the accumulator with
+// the cells outside it as zero.
 TPM_D void flush_tile(const float *acc, float *__restrict__ rho, int n, int ox, int oy, int oz, int vec4, int tid) {
+  constexpr int kUsed = kTile + 3;  // nodes [t-1, t+9] per axis
   if (vec4) {
-    for (int i = tid; i < kDepCells / 4; i += kDepThreads) {
-      int xq = i % (kDepNx / 4), r = i / (kDepNx / 4);
-      int y = r % kDepNy, z = r / kDepNy;
-      float4 v = *reinterpret_cast<const float4 *>(&acc[4 * xq + kDepNx * (y + kDepNy * z)]);
-      if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-      int gx = ox + 4 * xq, gy = oy + y, gz = oz + z;
+    for (int i = tid; i < 4 * kUsed * kUsed; i += kDepThreads) {
+      int q = i & 3, r = i >> 2;
+      int y = r % kUsed, z = r / kUsed;
+      const float *row = acc + kDepNx * (y + kDepNy * z);
+      float v[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        int xi = 4 * q - 3 + j;
+        v[j] = (xi >= 0 && xi < kUsed) ? row[xi] : 0.f;
+      }
+      if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f && v[3] == 0.f) continue;
+      int gx = ox - 3 + 4 * q, gy = oy + y, gz = oz + z;
       gx = (gx % n + n) % n;
       gy = (gy % n + n) % n;
       gz = (gz % n + n) % n;
       float4 *dst = reinterpret_cast<float4 *>(rho + gx + (int64_t)n * (gy + (int64_t)n * gz));
-      atomicAdd(dst, v);
+      atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
     }
   } else {
-    for (int i = tid; i < kDepCells; i += kDepThreads) {
-      float v = acc[i];
+    for (int i = tid; i < kUsed * kUsed * kUsed; i += kDepThreads) {
+      int x = i % kUsed, r = i / kUsed;
+      int y = r % kUsed, z = r / kUsed;
+      float v = acc[x + kDepNx * (y + kDepNy * z)];
       if (v == 0.f) continue;
-      int x = i % kDepNx, r = i / kDepNx;
-      int y = r % kDepNy, z = r / kDepNy;
       int gx = ((ox + x) % n + n) % n, gy = ((oy + y) % n + n) % n, gz = ((oz + z) % n + n) % n;
       atomicAdd(rho + gx + (int64_t)n * (gy + (int64_t)n * gz), v);
     }
@@ -191,7 +206,7 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
   }
   uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
   if (p0 == p1) return;
-  int ox = (int)tx * kTile - 4, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
+  int ox = (int)tx * kTile - 1, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
   for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0.f;
   __syncthreads();
   uint32_t nu = (uint32_t)n;
@@ -837,6 +852,11 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
 //   radius 2: the reference's 4-point stencil, 2/3 and -1/12 (fda4.c:45-46)
 //   radius 4: the 8-point stencil 4/5, -1/5, 4/105, -1/280 (the Gaussian law)
 constexpr int kNodes = kTile + 3;  // gradient nodes per axis
+// the gradient arrays' strides (1, 12, 144): the nodes of 32 Morton-
+// consecutive particles fall on distinct shared-memory banks
+constexpr int kGradSy = 12;
+constexpr int kGradSz = kGradSy * 12;
+constexpr int kGradSize = kGradSz * kNodes;
 constexpr int kFdaThreads = 256;
 
 template <int R>
@@ -877,8 +897,8 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
   extern __shared__ __align__(128) float fda_smem[];
   float(*box)[B::BY][B::BX] = reinterpret_cast<float(*)[B::BY][B::BX]>(fda_smem);
   float *gx = fda_smem + B::BY * B::BY * B::BX;
-  float *gy = gx + kNodes * kNodes * kNodes;
-  float *gz = gy + kNodes * kNodes * kNodes;
+  float *gy = gx + kGradSize;
+  float *gz = gy + kGradSize;
   __shared__ __align__(8) uint64_t bar;
   int tid = threadIdx.x;
   uint32_t t = blockIdx.x;
@@ -935,9 +955,10 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
       fz = c1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + c2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]) +
            c3 * (box[bz - 3][by][bx] - box[bz + 3][by][bx]) + c4 * (box[bz - 4][by][bx] - box[bz + 4][by][bx]);
     }
-    gx[i] = fx;
-    gy[i] = fy;
-    gz[i] = fz;
+    int gi = a + kGradSy * b + kGradSz * c;
+    gx[gi] = fx;
+    gy[gi] = fy;
+    gz[gi] = fz;
   }
   __syncthreads();
   uint32_t nu = (uint32_t)n;
@@ -963,7 +984,7 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
 #pragma unroll
         for (int a = 0; a < 3; a++) {
           float wt = wab[a] * wzs[c];
-          int node = ii[a] + kNodes * (jj[b] + kNodes * kk[c]);
+          int node = ii[a] + kGradSy * jj[b] + kGradSz * kk[c];
           fx += wt * gx[node];
           fy += wt * gy[node];
           fz += wt * gz[node];
@@ -1016,7 +1037,7 @@ int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorM
 void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
                  const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st, int half, int average) {
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
-  const size_t nodes = sizeof(float) * 3 * kNodes * kNodes * kNodes;
+  const size_t nodes = sizeof(float) * 3 * kGradSize;
   if (radius == 2) {
     size_t smem = sizeof(float) * FdaBox<2>::BY * FdaBox<2>::BY * FdaBox<2>::BX + nodes;
     cudaFuncSetAttribute(k_fda4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
