@@ -893,12 +893,11 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
                                                       uint32_t *__restrict__ err, uint32_t half, int average) {
   using B = FdaBox<R>;
   // dynamic shared memory: the potential box (128-byte aligned for TMA), then
-  // the three gradient components
+  // the gradient at the nodes as {-dphi/dx, -dphi/dy} pairs and -dphi/dz
   extern __shared__ __align__(128) float fda_smem[];
   float(*box)[B::BY][B::BX] = reinterpret_cast<float(*)[B::BY][B::BX]>(fda_smem);
-  float *gx = fda_smem + B::BY * B::BY * B::BX;
-  float *gy = gx + kGradSize;
-  float *gz = gy + kGradSize;
+  float2 *gxy = reinterpret_cast<float2 *>(fda_smem + B::BY * B::BY * B::BX);
+  float *gz = reinterpret_cast<float *>(gxy + kGradSize);
   __shared__ __align__(8) uint64_t bar;
   int tid = threadIdx.x;
   uint32_t t = blockIdx.x;
@@ -934,31 +933,44 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
     mbar_wait_bounded(&bar, 0, 1ll << 20);  // let an in-flight copy land before exit
     return;
   }
-  // gradient at nodes [t-1, t+T+1]^3
-  for (int i = tid; i < kNodes * kNodes * kNodes; i += kFdaThreads) {
-    int a = i % kNodes, r = i / kNodes;
-    int b = r % kNodes, c = r / kNodes;
-    // node (x0-1+a, y0-1+b, z0-1+c) -> box (a-1+X0, b-1+H, c-1+H)
-    int bx = a - 1 + B::X0, by = b - 1 + B::H, bz = c - 1 + B::H;
-    float fx, fy, fz;
-    if (R == 2) {
-      const float f1 = (4.f / 3.f) / 2.f, f2 = (-1.f / 3.f) / 4.f;
-      fx = f1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + f2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]);
-      fy = f1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + f2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]);
-      fz = f1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + f2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]);
+  // gradient at nodes [t-1, t+T+1]^3, one line of kNodes nodes per thread
+  // and axis: the line's kNodes + 2R potential values are read once and the
+  // differences taken in registers
+  constexpr int kLine = kNodes + 2 * R;
+  for (int r = tid; r < 3 * kNodes * kNodes; r += kFdaThreads) {
+    int axis = r / (kNodes * kNodes), rr = r % (kNodes * kNodes);
+    int p = rr % kNodes, q = rr / kNodes;
+    // node (a, b, c) sits at box (a-1+X0, b-1+H, c-1+H); v[i] is the line's
+    // value at node coordinate i - R
+    float v[kLine];
+    if (axis == 0) {
+#pragma unroll
+      for (int i = 0; i < kLine; i++) v[i] = box[q - 1 + B::H][p - 1 + B::H][B::X0 - 1 - R + i];
+    } else if (axis == 1) {
+#pragma unroll
+      for (int i = 0; i < kLine; i++) v[i] = box[q - 1 + B::H][B::H - 1 - R + i][p - 1 + B::X0];
     } else {
-      const float c1 = 4.f / 5.f, c2 = -1.f / 5.f, c3 = 4.f / 105.f, c4 = -1.f / 280.f;
-      fx = c1 * (box[bz][by][bx - 1] - box[bz][by][bx + 1]) + c2 * (box[bz][by][bx - 2] - box[bz][by][bx + 2]) +
-           c3 * (box[bz][by][bx - 3] - box[bz][by][bx + 3]) + c4 * (box[bz][by][bx - 4] - box[bz][by][bx + 4]);
-      fy = c1 * (box[bz][by - 1][bx] - box[bz][by + 1][bx]) + c2 * (box[bz][by - 2][bx] - box[bz][by + 2][bx]) +
-           c3 * (box[bz][by - 3][bx] - box[bz][by + 3][bx]) + c4 * (box[bz][by - 4][bx] - box[bz][by + 4][bx]);
-      fz = c1 * (box[bz - 1][by][bx] - box[bz + 1][by][bx]) + c2 * (box[bz - 2][by][bx] - box[bz + 2][by][bx]) +
-           c3 * (box[bz - 3][by][bx] - box[bz + 3][by][bx]) + c4 * (box[bz - 4][by][bx] - box[bz + 4][by][bx]);
+#pragma unroll
+      for (int i = 0; i < kLine; i++) v[i] = box[B::H - 1 - R + i][q - 1 + B::H][p - 1 + B::X0];
     }
-    int gi = a + kGradSy * b + kGradSz * c;
-    gx[gi] = fx;
-    gy[gi] = fy;
-    gz[gi] = fz;
+#pragma unroll
+    for (int a = 0; a < kNodes; a++) {
+      const float *w = v + a + R;
+      float f;
+      if (R == 2) {
+        const float f1 = (4.f / 3.f) / 2.f, f2 = (-1.f / 3.f) / 4.f;
+        f = f1 * (w[-1] - w[1]) + f2 * (w[-2] - w[2]);
+      } else {
+        const float c1 = 4.f / 5.f, c2 = -1.f / 5.f, c3 = 4.f / 105.f, c4 = -1.f / 280.f;
+        f = c1 * (w[-1] - w[1]) + c2 * (w[-2] - w[2]) + c3 * (w[-3] - w[3]) + c4 * (w[-4] - w[4]);
+      }
+      if (axis == 0)
+        gxy[a + kGradSy * p + kGradSz * q].x = f;
+      else if (axis == 1)
+        gxy[p + kGradSy * a + kGradSz * q].y = f;
+      else
+        gz[p + kGradSy * q + kGradSz * a] = f;
+    }
   }
   __syncthreads();
   uint32_t nu = (uint32_t)n;
@@ -985,8 +997,9 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
         for (int a = 0; a < 3; a++) {
           float wt = wab[a] * wzs[c];
           int node = ii[a] + kGradSy * jj[b] + kGradSz * kk[c];
-          fx += wt * gx[node];
-          fy += wt * gy[node];
+          float2 g = gxy[node];
+          fx += wt * g.x;
+          fy += wt * g.y;
           fz += wt * gz[node];
         }
       }
