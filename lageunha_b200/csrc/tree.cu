@@ -489,12 +489,12 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 
 // ------------------------------------------------------------------ walk
 constexpr int kWalkWarps = 16;
-constexpr int kWalkBlocksPerSm = 2;  // resident CTAs per SM the registers are budgeted for
+constexpr int kWalkBlocksPerSm = 1;  // resident CTAs per SM the registers are budgeted for
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kStackSmem = 640;    // per-warp stack entries in shared memory
 constexpr int kStackCap = 8192;    // entries beyond kStackSmem live in global memory
 constexpr int kPcCap = 64;
-constexpr int kPpBatch = 96;       // particle sources evaluated per flush
+constexpr int kPpBatch = 128;       // particle sources evaluated per flush
 constexpr int kLogSmemF4 = (kLogEntries + 2) / 2;  // the log-spaced table, in float4s
 
 struct WarpLists {
@@ -529,9 +529,13 @@ TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, const float2 *__
   float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
   uint32_t bits = __float_as_uint(r2);
-  int k = min((int)(bits >> kLogShift) - kLogBase, kLogEntries);
+  // entry (bits >> kLogShift) - kLogBase, the base folded into the shared
+  // address (s >= 2^-20 keeps the entry >= 0; the clamp keeps it in range)
+  uint32_t kk = min(bits >> kLogShift, (uint32_t)(kLogBase + kLogEntries));
   float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
-  float2 c = tl[k];
+  uint32_t tlb = (uint32_t)__cvta_generic_to_shared(tl) - (uint32_t)(kLogBase * 8);
+  float2 c;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
   float f = fmaf(c.y, m, c.x);
   if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
