@@ -38,6 +38,11 @@ struct tpm_ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[tpm::kNStages + 1];
+  // the PM chain of an evaluation that has both parts runs on st_pm, forked
+  // after the sort and joined before the walk, beside the tree build on st
+  cudaStream_t st_pm = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool overlapped = false;  // the last timed evaluation ran the two chains side by side
   // particles
   int64_t np = 0, cap = 0;
   uint32_t *pos = nullptr;

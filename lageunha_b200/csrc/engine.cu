@@ -545,6 +545,14 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
     return fail(TPM_E_CUDA, "cudaStreamCreate failed");
   }
   for (int i = 0; i <= kNStages; i++) cudaEventCreate(&c->ev[i]);
+  {
+    if (cudaStreamCreateWithFlags(&c->st_pm, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      tpm_destroy(c);
+      return fail(TPM_E_CUDA, "stream or event creation failed");
+    }
+  }
   // the allocations below are mirrored by ctx_bytes()
   if (cudaMalloc(&c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
       cudaMalloc(&c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
@@ -602,6 +610,9 @@ int tpm_destroy(tpm_ctx *c) {
   if (c->dfac) cudaFree(c->dfac);
   for (int i = 0; i <= kNStages; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st_pm) cudaStreamDestroy(c->st_pm);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return 0;
@@ -709,42 +720,51 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
   c->launches += 2;
   CK(stage_check(st, "sort"));
   if (timing) CK(cudaEventRecord(c->ev[1], st));
-  // ---- PM
+  // ---- PM: with both parts, on st_pm beside the tree build
+  bool split = (parts & TPM_PART_PM) && (parts & TPM_PART_TREE);
+  c->overlapped = split;
+  cudaStream_t pst = st;
+  if (split) {
+    CK(cudaEventRecord(c->ev_fork, st));
+    CK(cudaStreamWaitEvent(c->st_pm, c->ev_fork, 0));
+    pst = c->st_pm;
+  }
   if (parts & TPM_PART_PM) {
     uint32_t ntiles = 1u << (3 * (g.cbits - 3));
-    launch_range_table(c->skey, np, 3 * (g.sub_bits + 3), ntiles, c->tile_start, st);
-    CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
+    launch_range_table(c->skey, np, 3 * (g.sub_bits + 3), ntiles, c->tile_start, pst);
+    CK(cudaMemsetAsync(c->rho, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, pst));
     const bool il = c->prm.law == TPM_LAW_GAUSSIAN;  // interlaced pair of grids
-    if (il) CK(cudaMemsetAsync(c->rho2, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, st));
-    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, st, il ? c->rho2 : nullptr);
+    if (il) CK(cudaMemsetAsync(c->rho2, 0, sizeof(float) * (int64_t)g.n * g.n * g.n, pst));
+    launch_tsc_deposit(g, c->spos, c->tile_start, c->prm.particle_mass, c->rho, pst, il ? c->rho2 : nullptr);
     c->launches += 2;
-    CK(stage_check(st, "deposit"));
-    if (timing) CK(cudaEventRecord(c->ev[2], st));
+    CK(stage_check(pst, "deposit"));
+    if (timing) CK(cudaEventRecord(c->ev[2], pst));
     double *pk = c->measure_pk ? c->pk_acc : nullptr;
-    if (pk) CK(cudaMemsetAsync(pk, 0, sizeof(double) * 2 * (g.n + 1), st));
+    if (pk) CK(cudaMemsetAsync(pk, 0, sizeof(double) * 2 * (g.n + 1), pst));
     if (il)
-      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
+      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, pst,
                      &c->launches, c->rho2, c->spec2, c->phi2, c->gt, c->tune_fft_px, c->tune_fft_tx, pk);
     else
-      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, st,
+      launch_poisson(g, c->fp, c->rho, c->spec, c->phi, c->prm.law, c->prm.efold, c->prm.rs_split, pst,
                      &c->launches, nullptr, nullptr, nullptr, nullptr, c->tune_fft_px, c->tune_fft_tx, pk);
-    CK(stage_check(st, "fft"));
-    if (timing) CK(cudaEventRecord(c->ev[3], st));
+    CK(stage_check(pst, "fft"));
+    if (timing) CK(cudaEventRecord(c->ev[3], pst));
     // the reference law keeps the reference's 4-point gradient; the Gaussian
     // law uses the 8-point one on both interlaced grids and averages
     if (c->prm.law == TPM_LAW_REFERENCE) {
-      launch_fda4(g, &c->tmap2, 2, c->spos, c->tile_start, c->fpm, c->err, st);
+      launch_fda4(g, &c->tmap2, 2, c->spos, c->tile_start, c->fpm, c->err, pst);
       c->launches += 1;
     } else {
-      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, st, 0, 0);
-      launch_fda4(g, &c->tmap4b, 4, c->spos, c->tile_start, c->fpm, c->err, st, 1, 1);
+      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, pst, 0, 0);
+      launch_fda4(g, &c->tmap4b, 4, c->spos, c->tile_start, c->fpm, c->err, pst, 1, 1);
       c->launches += 2;
     }
-    CK(stage_check(st, "fda4"));
-    if (timing) CK(cudaEventRecord(c->ev[4], st));
+    CK(stage_check(pst, "fda4"));
+    if (timing) CK(cudaEventRecord(c->ev[4], pst));
   } else if (timing) {
-    for (int i = 2; i <= 4; i++) CK(cudaEventRecord(c->ev[i], st));
+    for (int i = 2; i <= 4; i++) CK(cudaEventRecord(c->ev[i], pst));
   }
+  if (split) CK(cudaEventRecord(c->ev_join, pst));
   // ---- tree
   if (parts & TPM_PART_TREE) {
     TreeParams tp;
@@ -761,6 +781,12 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
     int64_t gcubes = 1ll << (3 * (g.cbits - glev));
     tree_groups(tp, c->skey, np, c->tb, c->cube_start, gcubes, 3 * (g.sub_bits + glev), st, &c->launches);
     CK(stage_check(st, "tree_build"));
+    // the walk takes every SM: it starts once the PM chain is done too (the
+    // tree_build stage of an overlapped evaluation ends with both chains)
+    if (split) {
+      CK(cudaStreamWaitEvent(st, c->ev_join, 0));
+      split = false;
+    }
     if (timing) CK(cudaEventRecord(c->ev[5], st));
     if (walk) tree_walk(tp, c->spos, np, c->tb, c->law, c->ftree, c->err, st, &c->launches);
     CK(stage_check(st, "tree_walk"));
@@ -768,6 +794,7 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
   } else if (timing) {
     for (int i = 5; i <= 6; i++) CK(cudaEventRecord(c->ev[i], st));
   }
+  if (split) CK(cudaStreamWaitEvent(st, c->ev_join, 0));
   if (timing) CK(cudaEventRecord(c->ev[7], st));
   CK(cudaGetLastError());
   return 0;
@@ -790,8 +817,10 @@ int tpm::finish_forces(tpm_ctx *c, unsigned parts, bool from_host, bool timing) 
   }
   if (timing) {
     for (int s = 0; s < kNStages; s++) {
+      // beside the PM chain, the tree build starts at the end of the sort
+      int s0 = (s == kStTreeBuild && c->overlapped) ? kStDeposit : s;
       float ms = 0;
-      cudaEventElapsedTime(&ms, c->ev[s], c->ev[s + 1]);
+      cudaEventElapsedTime(&ms, c->ev[s0], c->ev[s + 1]);
       c->stage_ms[s] = ms;
     }
     // counters: nodes, pp, pc, groups
