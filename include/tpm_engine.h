@@ -368,6 +368,40 @@ int tpm_read_mesh(tpm_ctx *ctx, int which, float *out);
 
 /* ---- allocation-free ordering ---- */
 
+/* ---- Zel'dovich initial conditions (Cosmos/CosmosIC: PMSeedForce.c,
+ * Zeldovich.c, MakeParticle.c). One particle per point of an n^3 lattice,
+ * from the reference's random sequence (Numerical Recipes ran3/gasdev,
+ * CosmosIC/nr.c:317-384) in the reference's mode order, so a seed gives the
+ * reference's field. */
+typedef struct tpm_ic_params {
+  int32_t device;
+  int32_t n;            /* lattice points (= mesh cells) per side, 8..1024, 2^a 3^b 5^c */
+  int64_t iseed;        /* the reference's ISEED (PMSeedForce.c:219-223): >= 0 draws
+                           unit-amplitude noise with seed -1; < 0 draws with this seed,
+                           scaled by velpot */
+  const float *velpot;  /* host, (n/2)^2 + 1 floats: the amplitude pamp*bpower(rk)/rk^2 of
+                           PMSeedForce.c:326 at each integer k^2 = i^2 + ky^2 + kz^2
+                           (k in units of the fundamental mode); needed when iseed < 0 */
+  float fnl, gnl;       /* local non-Gaussianity (Zeldovich.c:44-61) */
+  float vamp;           /* growing-mode velocity factor COS_VAMP1 (PMSeedForce.c:250-292) */
+  float pfact;          /* offset per unit velocity, AI * NX (MakeParticle.c:205) */
+} tpm_ic_params;
+
+/* The noise spectrum of PMSeedForce.c:293-399 (one rank): spec receives
+ * n*n*(n/2+1) complex values (re, im floats), [z][y][kx]. Replaces the mode
+ * loop of PMSeedForce.c:293-334 and the conjugate completion of the kx = 0
+ * plane (PMSeedForce.c:346-399). */
+int tpm_ic_noise(const tpm_ic_params *p, float *spec, int mem);
+
+/* Zel'dovich particles: n^3 records of the reference's dark-matter layout
+ * (eunha.h:390-400, GOTPM with XYZDBL: 8-byte index i + n(j + n k), float
+ * offsets x y z, float velocities vx vy vz; 32 bytes each), in lattice
+ * order z, y, x. Velocity vamp * (vamp * psi) and offset pfact * velocity,
+ * psi the displacement of Zeldovich.c:14-100. Replaces Zeldovichmain
+ * (Zeldovichmain.c:28-84) for one rank with PORDER = 1. The records load
+ * with tpm_load_lagrangian. */
+int tpm_ic_zeldovich(const tpm_ic_params *p, void *records, int mem);
+
 /* Largest particle count tpm_morton_order_noalloc accepts: its scratch is a
  * fixed array of about 3.1 MB compiled into the library. */
 #define TPM_NOALLOC_MAX_PARTICLES 262144

@@ -68,6 +68,14 @@ struct FftPlan {
 };
 // twiddle tables are written on st
 void fft_plan_init(FftPlan &p, int n, cudaStream_t st);
+// plain unnormalised transforms: real [z][y][x] -> spec [z][y][hx] (e^{-i}),
+// spec -> ghosted real (e^{+i}; spec is overwritten)
+void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 *spec, cudaStream_t st);
+void fft_inverse(const MeshGeom &g, const FftPlan &p, float2 *spec, float *phi_pad, cudaStream_t st);
+// exclusive scan of n u32 values: out[i] = local prefix within blocks of
+// 4096, bsum[i / 4096] = the block's offset (bsum holds (n + 4095) / 4096
+// entries), *total = the sum
+void scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *bsum, uint32_t *total, cudaStream_t st);
 void fft_plan_free(FftPlan &p);
 // With rho2 (the half-cell-shifted deposit) the two grids are interlaced:
 // their spectra are combined before the Green's function and phi2_pad gets

@@ -11,6 +11,7 @@
 //   ghosted potential      Cosmos/pmmain.c:337-388
 //   gradient + interp.     Cosmos/fda4.h:11-103,276-384, fda4.c:45-46
 #include <math.h>
+#include <string.h>
 #include <stdio.h>
 
 #include <algorithm>
@@ -843,6 +844,49 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
     k_fft_x_c2r<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(spec2, phi2_pad, ax, twL, p.tw, nrows,
                                                                        g.px, g.py);
   if (launches) *launches += rho2 ? 7 : 5;
+}
+
+// Plain transforms of an n^3 mesh with the same kernels (no Green's
+// function, unnormalised): forward = x r2c, y and z passes with e^{-i};
+// inverse = z and y passes with e^{+i}, x c2r into the ghosted layout.
+void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 *spec, cudaStream_t st) {
+  int n = g.n;
+  int64_t nrows = (int64_t)n * n;
+  bool packed = (n % 2) == 0;
+  int Lx = packed ? n / 2 : n;
+  int Px = pencils_for(Lx);
+  FftArgs ax = fft_args(n, Lx, Px);
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), 256, smx, st>>>(real, spec, ax, packed ? p.tw_half : p.tw,
+                                                                   p.tw, nrows);
+  int TX = cols_per_block(n, g.hx, 1);
+  FftArgs ac = fft_args(n, n, TX);
+  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  int ntx = (g.hx + TX - 1) / TX;
+  GreenArgs ga;
+  memset(&ga, 0, sizeof(ga));
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, nullptr, ac, p.tw, 1, -1.f, 0, ga, TX, 1);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, nullptr, ac, p.tw, 2, -1.f, 0, ga, TX, 1);
+}
+
+void fft_inverse(const MeshGeom &g, const FftPlan &p, float2 *spec, float *phi_pad, cudaStream_t st) {
+  int n = g.n;
+  int64_t nrows = (int64_t)n * n;
+  bool packed = (n % 2) == 0;
+  int Lx = packed ? n / 2 : n;
+  int Px = pencils_for(Lx);
+  FftArgs ax = fft_args(n, Lx, Px);
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  int TX = cols_per_block(n, g.hx, 1);
+  FftArgs ac = fft_args(n, n, TX);
+  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  int ntx = (g.hx + TX - 1) / TX;
+  GreenArgs ga;
+  memset(&ga, 0, sizeof(ga));
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, nullptr, ac, p.tw, 2, 1.f, 0, ga, TX, 1);
+  k_fft_cols<<<(unsigned)(n * ntx), 256, smc, st>>>(spec, nullptr, ac, p.tw, 1, 1.f, 0, ga, TX, 1);
+  k_fft_x_c2r<<<(unsigned)((nrows + Px - 1) / Px), 256, smx, st>>>(spec, phi_pad, ax, packed ? p.tw_half : p.tw,
+                                                                   p.tw, nrows, g.px, g.py);
 }
 
 // ------------------------------------------------------------------ fda4

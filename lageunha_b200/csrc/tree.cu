@@ -468,6 +468,12 @@ __global__ void k_write_groups(const uint32_t *__restrict__ cube_start, int64_t 
   }
 }
 
+void scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *bsum, uint32_t *total, cudaStream_t st) {
+  int64_t nb = (n + 4095) / 4096;
+  k_scan_block<<<(unsigned)nb, 1024, 0, st>>>(in, out, n, bsum);
+  k_scan_sums<<<1, 1024, 0, st>>>(bsum, nb, total);
+}
+
 void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuffers &tb,
                  uint32_t *cube_start, int64_t ncubes, int cube_shift, cudaStream_t st,
                  int64_t *launches) {

@@ -93,6 +93,12 @@ class TpmSnapshotInfo(ctypes.Structure):
         [("stepcount", ctypes.c_int32), ("data_offset", ctypes.c_int64)]
 
 
+class TpmIcParams(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("n", ctypes.c_int32), ("iseed", ctypes.c_int64),
+                ("velpot", ctypes.c_void_p), ("fnl", ctypes.c_float), ("gnl", ctypes.c_float),
+                ("vamp", ctypes.c_float), ("pfact", ctypes.c_float)]
+
+
 class EngineError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"tpm error {code}: {msg}")
@@ -160,6 +166,8 @@ _SIGS = {
                                         ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
     "tpm_hubble_drag": (ctypes.c_int, [_P, ctypes.c_float]),
     "tpm_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float, ctypes.c_int32]),
+    "tpm_ic_noise": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
+    "tpm_ic_zeldovich": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
 }
 
 
@@ -592,3 +600,39 @@ def treedm_records(ps) -> np.ndarray:
     r["x"], r["y"], r["z"] = ps.offset[:, 0], ps.offset[:, 1], ps.offset[:, 2]
     r["vx"], r["vy"], r["vz"] = ps.vel[:, 0], ps.vel[:, 1], ps.vel[:, 2]
     return r
+
+
+def _ic_params(n, iseed, velpot, fnl, gnl, vamp, pfact, device):
+    p = TpmIcParams()
+    p.device, p.n, p.iseed = device, n, iseed
+    p.fnl, p.gnl, p.vamp, p.pfact = fnl, gnl, vamp, pfact
+    keep = None
+    if velpot is not None:
+        keep = np.ascontiguousarray(velpot, dtype=np.float32)
+        if keep.shape[0] < (n // 2) ** 2 + 1:
+            raise ValueError("velpot needs (n/2)^2 + 1 entries")
+        p.velpot = keep.ctypes.data
+    return p, keep
+
+
+def ic_noise(n: int, iseed: int, velpot=None, device: int = 0) -> np.ndarray:
+    """The reference's Zel'dovich noise spectrum (tpm_ic_noise) as complex64
+    [z][y][kx], kx in [0, n/2]."""
+    lib = load_library()
+    p, keep = _ic_params(n, iseed, velpot, 0.0, 0.0, 1.0, 1.0, device)
+    out = np.empty((n, n, n // 2 + 1), np.complex64)
+    _check(lib.tpm_ic_noise(ctypes.byref(p), out.ctypes.data, MEM_HOST))
+    del keep
+    return out
+
+
+def ic_zeldovich(n: int, iseed: int, velpot=None, fnl: float = 0.0, gnl: float = 0.0, vamp: float = 1.0,
+                 pfact: float | None = None, device: int = 0) -> np.ndarray:
+    """Zel'dovich particles (tpm_ic_zeldovich): n^3 DM_DTYPE records, lattice
+    order z, y, x; pfact defaults to the reference's AI * NX = n."""
+    lib = load_library()
+    p, keep = _ic_params(n, iseed, velpot, fnl, gnl, vamp, float(n if pfact is None else pfact), device)
+    rec = np.empty(n ** 3, DM_DTYPE)
+    _check(lib.tpm_ic_zeldovich(ctypes.byref(p), rec.ctypes.data, MEM_HOST))
+    del keep
+    return rec

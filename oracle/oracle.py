@@ -297,3 +297,77 @@ def morton_keys(pos_u32, n):
 def sort_order(keys):
     """The engine's permutation: stable argsort (ties keep input order)."""
     return np.argsort(keys, kind="stable")
+
+
+# ---------------------------------------------------------------- initial conditions
+def _ran3_stream(idum):
+    """Numerical Recipes ran3 (Cosmos/CosmosIC/nr.c:317-355) as a generator of
+    the integer states mj; ran3's float is float32(mj * 1e-9)."""
+    mbig, mseed = 1000000000, 161803398
+    ma = [0] * 56
+    mj = (mseed - abs(idum)) % mbig
+    ma[55] = mj
+    mk = 1
+    for i in range(1, 55):
+        ii = (21 * i) % 55
+        ma[ii] = mk
+        mk = mj - mk
+        if mk < 0:
+            mk += mbig
+        mj = ma[ii]
+    for _ in range(4):
+        for i in range(1, 56):
+            ma[i] -= ma[1 + (i + 30) % 55]
+            if ma[i] < 0:
+                ma[i] += mbig
+    inext, inextp = 0, 31
+    while True:
+        inext = 1 if inext + 1 == 56 else inext + 1
+        inextp = 1 if inextp + 1 == 56 else inextp + 1
+        mj = ma[inext] - ma[inextp]
+        if mj < 0:
+            mj += mbig
+        ma[inext] = mj
+        yield mj
+
+
+def gasdev_pairs(idum, count):
+    """The first `count` accepted pairs of gasdev (nr.c:361-384) on ran3, in
+    the order gasdev returns them (v2*fac, v1*fac), with the C float and
+    double rounding of each operation. A restatement for small counts."""
+    f32 = np.float32
+    st = _ran3_stream(idum)
+    out = np.empty((count, 2), np.float32)
+    k = 0
+    while k < count:
+        v1 = f32(2.0 * float(f32(next(st) * (1.0 / 1e9))) - 1.0)
+        v2 = f32(2.0 * float(f32(next(st) * (1.0 / 1e9))) - 1.0)
+        rsq = f32(f32(v1 * v1) + f32(v2 * v2))
+        if rsq >= 1.0 or rsq == 0.0:
+            continue
+        fac = f32(np.sqrt(-2.0 * np.log(float(rsq)) / float(rsq)))
+        out[k] = (f32(v2 * fac), f32(v1 * fac))
+        k += 1
+    return out
+
+
+def ref_ic_noise(n, iseed, velpot=None):
+    """The reference's noise spectrum for one rank (ref_shim.c ref_ic_noise:
+    PMSeedForce's mode loop and conjugate completion on the reference's own
+    gasdev/ran3): complex64 [z][y][kx]."""
+    den = np.zeros((n, n, 2 * (n // 2 + 1)), np.float32)
+    vp = None if velpot is None else np.ascontiguousarray(velpot, np.float32)
+    ref(VARIANT_A).ref_ic_noise(ctypes.c_int(n), ctypes.c_long(iseed),
+                                None if vp is None else vp.ctypes.data_as(ctypes.c_void_p),
+                                den.ctypes.data_as(ctypes.c_void_p))
+    return den.view(np.complex64)
+
+
+def ref_zeldovich(n, den, fnl=0.0, gnl=0.0):
+    """The reference's Zeldovich (Cosmos/CosmosIC/Zeldovich.c) on a noise
+    spectrum: (fx, fy, fz) displacement fields as float32 [z][y][x]."""
+    d = np.ascontiguousarray(den, np.complex64).view(np.float32).reshape(n, n, 2 * (n // 2 + 1)).copy()
+    f = [np.zeros_like(d) for _ in range(3)]
+    ref(VARIANT_A).ref_zeldovich(ctypes.c_int(n), ctypes.c_float(fnl), ctypes.c_float(gnl),
+                                 d.ctypes.data_as(ctypes.c_void_p), *[a.ctypes.data_as(ctypes.c_void_p) for a in f])
+    return tuple(a[:, :, :n] for a in f)

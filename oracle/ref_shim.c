@@ -77,10 +77,13 @@ int MPI_Comm_size(MPI_Comm c, int *s) { (void)c; *s = 1; return 0; }
 /* --------------------------------------------------------- FFTW-MPI shim */
 struct fftwf_plan_s {
   ptrdiff_t n0, n1, n2; /* z, y, x */
+  int natural;          /* 1: the plans without FFTW_MPI_TRANSPOSED_* (FFT/fft.c:81-94, the IC's
+                           np/inp): spectrum stored as [z][y][kx] */
 };
 
 void fftwf_mpi_execute_dft_r2c(fftwf_plan p, float *in, fftwf_complex *out) {
   ptrdiff_t nz = p->n0, ny = p->n1, nx = p->n2, hx = nx / 2 + 1, mx = 2 * hx;
+  int nat = p->natural;
   double *r = (double *)malloc(sizeof(double) * nx * ny * nz);
   double *c = (double *)malloc(sizeof(double) * 2 * hx * ny * nz);
   for (ptrdiff_t k = 0; k < nz; k++)
@@ -93,7 +96,7 @@ void fftwf_mpi_execute_dft_r2c(fftwf_plan p, float *in, fftwf_complex *out) {
     for (ptrdiff_t j = 0; j < ny; j++)
       for (ptrdiff_t i = 0; i < hx; i++) {
         size_t src = 2 * (i + hx * (j + ny * k));
-        size_t dst = 2 * (i + hx * (k + nz * j));
+        size_t dst = nat ? src : 2 * (i + hx * (k + nz * j));
         o[dst] = (float)c[src];
         o[dst + 1] = (float)c[src + 1];
       }
@@ -103,6 +106,7 @@ void fftwf_mpi_execute_dft_r2c(fftwf_plan p, float *in, fftwf_complex *out) {
 
 void fftwf_mpi_execute_dft_c2r(fftwf_plan p, fftwf_complex *in, float *out) {
   ptrdiff_t nz = p->n0, ny = p->n1, nx = p->n2, hx = nx / 2 + 1, mx = 2 * hx;
+  int nat = p->natural;
   double *c = (double *)malloc(sizeof(double) * 2 * hx * ny * nz);
   double *r = (double *)malloc(sizeof(double) * nx * ny * nz);
   const float *ci = (const float *)in;
@@ -110,7 +114,7 @@ void fftwf_mpi_execute_dft_c2r(fftwf_plan p, fftwf_complex *in, float *out) {
     for (ptrdiff_t j = 0; j < ny; j++)
       for (ptrdiff_t i = 0; i < hx; i++) {
         size_t dst = 2 * (i + hx * (j + ny * k));
-        size_t src = 2 * (i + hx * (k + nz * j));
+        size_t src = nat ? dst : 2 * (i + hx * (k + nz * j));
         c[dst] = ci[src];
         c[dst + 1] = ci[src + 1];
       }
@@ -226,7 +230,7 @@ void i_force_spline(SimParameters *);
 typedef struct {
   SimParameters sim;
   DoDeInfo dd;
-  struct fftwf_plan_s fplan, bplan;
+  struct fftwf_plan_s fplan, bplan, nfplan, nbplan;
 } RefBox;
 
 static RefBox *refbox_new(int n, float efold, float eps, float theta, float rsphere) {
@@ -246,8 +250,13 @@ static RefBox *refbox_new(int n, float efold, float eps, float theta, float rsph
   LOCAL_Y_START_AFTER_TRANSPOSE(s) = 0;
   b->fplan.n0 = b->fplan.n1 = b->fplan.n2 = n;
   b->bplan = b->fplan;
+  b->nfplan = b->fplan;
+  b->nfplan.natural = 1;
+  b->nbplan = b->nfplan;
   FFTW_F_PLAN(s) = &b->fplan;
   FFTW_B_PLAN(s) = &b->bplan;
+  FFTW_NF_PLAN(s) = &b->nfplan;
+  FFTW_NB_PLAN(s) = &b->nbplan;
   for (int d = 0; d < 3; d++) {
     b->dd.lgroup.r.rmin[d] = 0;
     b->dd.lgroup.r.rmax[d] = n;
@@ -509,4 +518,91 @@ int ref_power_spectrum(int n, int64_t np, const uint64_t *indx, const float *off
   int rc = ref_pm_force(n, np, indx, off, 0.9f, force);
   g_corr = 0;
   return rc;
+}
+
+/* ---------------------------------------------------------- initial conditions
+ * The white-noise field of the Zel'dovich initial conditions for one rank:
+ * the mode loop of PMSeedForce (Cosmos/CosmosIC/PMSeedForce.c:293-334) with
+ * the reference's own gasdev/ran3 (Cosmos/CosmosIC/nr.c:317-384), and its
+ * completion of the kx = 0 plane by complex conjugates (PMSeedForce.c:346-399,
+ * where the per-rank columns gathered into denpad are, with one rank, the
+ * kx = 0 column of den itself). The Fortran amplitude pamp*bpower(rk)/rk^2 of
+ * the P(k)-weighted path is passed in as its value per integer
+ * k^2 = i^2 + ky^2 + kz^2 (velpot_k2[k2], k2 <= (n/2)^2); iseed >= 0 is the
+ * reference's unit-amplitude path, which always runs with seed -1.
+ * den: n*n*2*(n/2+1) floats, [z][y][2*(n/2+1)] (the non-transposed layout the
+ * IC's plans use). */
+float gasdev(long *);
+int ref_ic_noise(int n, long iseed, const float *velpot_k2, float *den) {
+  ptrdiff_t nx = n, ny = n, nz = n, mx = 2 * (nx / 2 + 1);
+  int seedflag = 0;
+  if (iseed >= 0) {
+    seedflag = 1;
+    iseed = -1;
+  }
+  long iiseed = iseed;
+  double rknyq2 = (double)(nx / 2) * (double)(nx / 2);
+  for (ptrdiff_t k = 0; k < nz; k++) {
+    ptrdiff_t kz = k > nz / 2 ? k - nz : k;
+    for (ptrdiff_t j = 0; j < ny; j++) {
+      ptrdiff_t ky = j > ny / 2 ? j - ny : j;
+      for (ptrdiff_t i = 0; i <= nx / 2; i++) {
+        double xksq = (double)(i * i + ky * ky + kz * kz);
+        float *d = den + 2 * i + mx * (j + ny * k);
+        if (xksq == 0 || xksq > rknyq2) {
+          d[0] = 0;
+          d[1] = 0;
+        } else if (seedflag) {
+          d[0] = gasdev(&iiseed);
+          d[1] = gasdev(&iiseed);
+        } else {
+          float velpot = velpot_k2[(ptrdiff_t)xksq];
+          d[0] = velpot * gasdev(&iiseed);
+          d[1] = velpot * gasdev(&iiseed);
+        }
+      }
+    }
+  }
+  /* kx = 0 column: (re, im) at den[mx*(j+ny*k)] */
+#define C0(j, k) (den + mx * ((j) + ny * (k)))
+  for (ptrdiff_t k = 1; k < nz / 2; k++) {
+    C0(0, nz - k)[0] = C0(0, k)[0];
+    C0(0, nz - k)[1] = -C0(0, k)[1];
+    for (ptrdiff_t j = 1; j < ny / 2; j++) {
+      C0(ny - j, nz - k)[0] = C0(j, k)[0];
+      C0(ny - j, nz - k)[1] = -C0(j, k)[1];
+    }
+  }
+  for (ptrdiff_t j = 1; j < ny / 2; j++) {
+    C0(ny - j, 0)[0] = C0(j, 0)[0];
+    C0(ny - j, 0)[1] = -C0(j, 0)[1];
+  }
+  for (ptrdiff_t k = 1; k < nz / 2; k++)
+    for (ptrdiff_t j = ny / 2 + 1; j < ny; j++) {
+      C0(ny - j, nz - k)[0] = C0(j, k)[0];
+      C0(ny - j, nz - k)[1] = -C0(j, k)[1];
+    }
+#undef C0
+  return 0;
+}
+
+/* The reference's Zeldovich (Cosmos/CosmosIC/Zeldovich.c:14-100) on one rank:
+ * den in/out (the noise field above; left as the potential's spectrum after
+ * the fNL/gNL step), fx/fy/fz the displacement fields in the padded real
+ * layout [z][y][2*(n/2+1)]. fx/fy/fz are cleared first: the reference fills
+ * their spectra for kx < n/2 only (Zeldovich.c:71-88), leaving the kx = n/2
+ * plane as it found it. */
+void Zeldovich(SimParameters *, DenType *, DenType *, DenType *, DenType *);
+int ref_zeldovich(int n, float fnl, float gnl, float *den, float *fx, float *fy, float *fz) {
+  RefBox *b = refbox_new(n, 0.9f, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  FNL(s) = fnl;
+  GNL(s) = gnl;
+  size_t sz = (size_t)n * n * 2 * (n / 2 + 1);
+  memset(fx, 0, sizeof(float) * sz);
+  memset(fy, 0, sizeof(float) * sz);
+  memset(fz, 0, sizeof(float) * sz);
+  Zeldovich(s, den, fx, fy, fz);
+  free(b);
+  return 0;
 }
