@@ -627,11 +627,20 @@ def ic_noise(n: int, iseed: int, velpot=None, device: int = 0) -> np.ndarray:
 
 
 def ic_zeldovich(n: int, iseed: int, velpot=None, fnl: float = 0.0, gnl: float = 0.0, vamp: float = 1.0,
-                 pfact: float | None = None, device: int = 0) -> np.ndarray:
+                 pfact: float | None = None, device: int = 0, out=None):
     """Zel'dovich particles (tpm_ic_zeldovich): n^3 DM_DTYPE records, lattice
-    order z, y, x; pfact defaults to the reference's AI * NX = n."""
+    order z, y, x; pfact defaults to the reference's AI * NX = n. `out`: a
+    device tensor of n^3 * 32 bytes to receive the records instead of a new
+    host array."""
     lib = load_library()
     p, keep = _ic_params(n, iseed, velpot, fnl, gnl, vamp, float(n if pfact is None else pfact), device)
+    if out is not None:
+        if out.numel() * out.element_size() < n ** 3 * DM_DTYPE.itemsize:
+            raise ValueError("out is smaller than n^3 records")
+        ptr, mem = _ptr(out)
+        _check(lib.tpm_ic_zeldovich(ctypes.byref(p), ptr, mem))
+        del keep
+        return out
     rec = np.empty(n ** 3, DM_DTYPE)
     _check(lib.tpm_ic_zeldovich(ctypes.byref(p), rec.ctypes.data, MEM_HOST))
     del keep

@@ -255,3 +255,62 @@ def workload(name: str, scale: int | None = None, device: str | None = None) -> 
         return zeldovich(n, seed=3, spec_index=-2.5, damp=0.5, rms_disp=2.0, box_mpc=500.0, vel_factor=0.5,
                          device=device)
     raise KeyError(name)
+
+
+# ---------------------------------------------------------------- amplitude tables
+# The reference scales each noise mode of its initial conditions by
+# pamp*bpower(rk)/rk^2 (Cosmos/CosmosIC/PMSeedForce.c:326), with bpower the
+# square root of the CAMB power spectrum in its units (P(k) = (pamp bpower)^2
+# boxsize^3, PMSeedForce.c:296-297), pamp normalising the top-hat variance at
+# 8 Mpc/h to 1/bias, times the growth ratio bini/bnow and N^3 sqrt(1/2)
+# (PMSeedForce.c:250-295). Its bpower and the normalising integral are
+# Fortran (CosmosIC/sub.lynx.camb.F), which this image cannot compile; the
+# table below is built from the same definitions by this module.
+
+def read_pk_table(path: str):
+    """(k [h/Mpc], P(k) [(Mpc/h)^3]) from a whitespace-separated two-column
+    file such as CAMB's matter power output."""
+    a = np.loadtxt(path, usecols=(0, 1), ndmin=2)
+    return a[:, 0].astype(np.float64), a[:, 1].astype(np.float64)
+
+
+def _pk_interp(k_tab, p_tab, k):
+    """Log-log interpolation of the table, power-law continued past its ends."""
+    lk, lp = np.log(k_tab), np.log(p_tab)
+    x = np.log(np.maximum(k, 1e-30))
+    y = np.interp(x, lk, lp)
+    lo, hi = x < lk[0], x > lk[-1]
+    if lo.any():
+        s = (lp[1] - lp[0]) / (lk[1] - lk[0])
+        y[lo] = lp[0] + s * (x[lo] - lk[0])
+    if hi.any():
+        s = (lp[-1] - lp[-2]) / (lk[-1] - lk[-2])
+        y[hi] = lp[-1] + s * (x[hi] - lk[-1])
+    return np.exp(y)
+
+
+def sigma_tophat(k_tab, p_tab, radius: float = 8.0) -> float:
+    """rms density contrast in a top-hat sphere of `radius` Mpc/h:
+    sigma^2 = 1/(2 pi^2) int k^2 P(k) W(kR)^2 dk, W(x) = 3 (sin x - x cos x)/x^3
+    (the integrand of the reference's bpowint, sub.lynx.camb.F:214-228)."""
+    k = np.exp(np.linspace(np.log(1e-4), np.log(1e2), 20001))
+    x = k * radius
+    w = np.where(x > 0.02, 3 * (np.sin(x) - x * np.cos(x)) / np.maximum(x, 1e-30) ** 3, 1 - x * x / 10)
+    f = k ** 3 * _pk_interp(k_tab, p_tab, k) * w * w
+    return float(np.sqrt(np.trapezoid(f, np.log(k)) / (2 * np.pi ** 2)))
+
+
+def velpot_table(n: int, boxsize: float, k_tab, p_tab, growth: float = 1.0, sigma8: float | None = None):
+    """The per-k^2 amplitude tpm_ic_zeldovich takes: growth * N^3 sqrt(1/2)
+    sqrt(P(k)/L^3) / rk^2 at rk = 2 pi sqrt(k^2), k = rk / L, for integer
+    k^2 <= (n/2)^2; with sigma8 the table's P(k) is first scaled to that
+    top-hat rms at 8 Mpc/h. growth is D(a_initial)/D(a_final)."""
+    p_tab = np.asarray(p_tab, np.float64)
+    if sigma8 is not None:
+        p_tab = p_tab * (sigma8 / sigma_tophat(k_tab, p_tab)) ** 2
+    k2 = np.arange((n // 2) ** 2 + 1, dtype=np.float64)
+    rk = 2 * np.pi * np.sqrt(np.maximum(k2, 1.0))
+    pk = _pk_interp(np.asarray(k_tab, np.float64), p_tab, rk / boxsize)
+    v = growth * float(n) ** 3 * np.sqrt(0.5) * np.sqrt(pk / boxsize ** 3) / rk ** 2
+    v[0] = 0.0
+    return v.astype(np.float32)

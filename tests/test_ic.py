@@ -60,6 +60,20 @@ def power_law_velpot(n, slope=-2.0, amp=0.05):
     return (amp * rk ** (slope / 2) / rk ** 2 * n ** 3).astype(np.float32)
 
 
+def test_velpot_table_normalisation():
+    from lageunha_b200 import ic
+    k = np.exp(np.linspace(np.log(1e-3), np.log(50), 400))
+    p = 2e4 * (k / 0.02) / (1 + (k / 0.02) ** 3)
+    # scaling to sigma_8 scales the table by sigma_8 / sigma_8(table)
+    s = ic.sigma_tophat(k, p)
+    v1 = ic.velpot_table(32, 100.0, k, p)
+    v2 = ic.velpot_table(32, 100.0, k, p, sigma8=2 * s)
+    assert np.allclose(v2[1:], 2 * v1[1:], rtol=1e-6) and v1[0] == 0
+    # a power law P = A / k gives velpot ~ k2^(-1/4) / k2 = k2^(-5/4)
+    v = ic.velpot_table(64, 100.0, k, 3.0 / k)
+    assert np.allclose(v[16] / v[4], (16 / 4) ** -1.25, rtol=1e-5)
+
+
 def test_ran3_known_answers():
     # ran3 with idum = -1: its state after initialisation gives these first
     # draws (the restatement above), checked against the reference below
@@ -162,3 +176,27 @@ def test_bad_ic_arguments():
         E.ic_noise(14, 3)            # 14 = 2 * 7
     with pytest.raises(E.EngineError):
         E.ic_noise(16, -3, None)     # a weighted seed needs the table
+
+
+@pytest.mark.gpu
+def test_ic_power_spectrum_follows_the_table():
+    """End to end: particles from a CAMB-like table (sigma_8 = 0.8 at 8 Mpc/h,
+    growth 1/50) in a 200 Mpc/h box at 64^3, measured with the engine's
+    CorrMeasure P(k) (per unit box volume): times L^3 it follows the table
+    times growth^2 within the cosmic variance of the bins."""
+    from lageunha_b200 import ic
+    n, L, g = 64, 200.0, 1.0 / 50
+    k = np.exp(np.linspace(np.log(1e-3), np.log(50), 400))
+    p = 2e4 * (k / 0.02) / (1 + (k / 0.02) ** 3)
+    rec = E.ic_zeldovich(n, -31, ic.velpot_table(n, L, k, p, growth=g, sigma8=0.8))
+    with E.Engine(n, epsilon=0.05) as eng:
+        eng.load_lagrangian(rec)
+        eng.measure_power_spectrum(True)
+        eng.compute(E.PART_PM)
+        r = eng.power_spectrum(L)
+    p8 = p * (0.8 / ic.sigma_tophat(k, p)) ** 2
+    bins = np.arange(2, 13)
+    want = g * g * ic._pk_interp(k, p8, 2 * np.pi * bins / L)
+    ratio = r["pk"][bins] * L ** 3 / want
+    assert np.all((ratio > 0.8) & (ratio < 1.25)), ratio
+    assert abs(float(np.mean(ratio)) - 1.0) < 0.1, ratio
