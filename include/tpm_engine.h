@@ -385,6 +385,9 @@ typedef struct tpm_ic_params {
   float fnl, gnl;       /* local non-Gaussianity (Zeldovich.c:44-61) */
   float vamp;           /* growing-mode velocity factor COS_VAMP1 (PMSeedForce.c:250-292) */
   float pfact;          /* offset per unit velocity, AI * NX (MakeParticle.c:205) */
+  /* second order only (tpm_ic_2lpt): COS_VAMP2, COS_DAMP1, COS_DAMP2
+     (PMSeedForce.c:250-305; damp1 = 1, damp2 = -3/7 in the reference) */
+  float vamp2, damp1, damp2;
 } tpm_ic_params;
 
 /* The noise spectrum of PMSeedForce.c:293-399 (one rank): spec receives
@@ -401,6 +404,14 @@ int tpm_ic_noise(const tpm_ic_params *p, float *spec, int mem);
  * (Zeldovichmain.c:28-84) for one rank with PORDER = 1. The records load
  * with tpm_load_lagrangian. */
 int tpm_ic_zeldovich(const tpm_ic_params *p, void *records, int mem);
+
+/* Second-order Lagrangian particles (PORDER = 2): TwoLPTmain
+ * (Cosmos/CosmosIC/TwoLPTmain.c:157-240) for one rank. The second-order
+ * potential of TwoLPT (TwoLPT.c:259-535) from the same noise; velocity
+ * d/dx (vamp phi1 + vamp2 phi2) and offset d/dx (pfact damp1 phi1 +
+ * pfact damp2 phi2) per axis (TwoLPT_GetVR, cosmosic.h:141-163). Same
+ * records as tpm_ic_zeldovich; fnl and gnl must be 0. */
+int tpm_ic_2lpt(const tpm_ic_params *p, void *records, int mem);
 
 /* Largest particle count tpm_morton_order_noalloc accepts: its scratch is a
  * fixed array of about 3.1 MB compiled into the library. */

@@ -96,7 +96,8 @@ class TpmSnapshotInfo(ctypes.Structure):
 class TpmIcParams(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("n", ctypes.c_int32), ("iseed", ctypes.c_int64),
                 ("velpot", ctypes.c_void_p), ("fnl", ctypes.c_float), ("gnl", ctypes.c_float),
-                ("vamp", ctypes.c_float), ("pfact", ctypes.c_float)]
+                ("vamp", ctypes.c_float), ("pfact", ctypes.c_float), ("vamp2", ctypes.c_float),
+                ("damp1", ctypes.c_float), ("damp2", ctypes.c_float)]
 
 
 class EngineError(RuntimeError):
@@ -168,6 +169,7 @@ _SIGS = {
     "tpm_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float, ctypes.c_int32]),
     "tpm_ic_noise": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
     "tpm_ic_zeldovich": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
+    "tpm_ic_2lpt": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
 }
 
 
@@ -643,5 +645,17 @@ def ic_zeldovich(n: int, iseed: int, velpot=None, fnl: float = 0.0, gnl: float =
         return out
     rec = np.empty(n ** 3, DM_DTYPE)
     _check(lib.tpm_ic_zeldovich(ctypes.byref(p), rec.ctypes.data, MEM_HOST))
+    del keep
+    return rec
+
+
+def ic_2lpt(n: int, iseed: int, velpot=None, vamp: float = 1.0, vamp2: float = 0.0, damp1: float = 1.0,
+            damp2: float = -3.0 / 7.0, pfact: float | None = None, device: int = 0) -> np.ndarray:
+    """Second-order Lagrangian particles (tpm_ic_2lpt): n^3 DM_DTYPE records."""
+    lib = load_library()
+    p, keep = _ic_params(n, iseed, velpot, 0.0, 0.0, vamp, float(n if pfact is None else pfact), device)
+    p.vamp2, p.damp1, p.damp2 = vamp2, damp1, damp2
+    rec = np.empty(n ** 3, DM_DTYPE)
+    _check(lib.tpm_ic_2lpt(ctypes.byref(p), rec.ctypes.data, MEM_HOST))
     del keep
     return rec

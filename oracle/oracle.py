@@ -371,3 +371,16 @@ def ref_zeldovich(n, den, fnl=0.0, gnl=0.0):
     ref(VARIANT_A).ref_zeldovich(ctypes.c_int(n), ctypes.c_float(fnl), ctypes.c_float(gnl),
                                  d.ctypes.data_as(ctypes.c_void_p), *[a.ctypes.data_as(ctypes.c_void_p) for a in f])
     return tuple(a[:, :, :n] for a in f)
+
+
+def ref_two_lpt(n, den, amp1, amp2, vamp1, vamp2):
+    """The reference's second-order initial conditions for one rank (TwoLPT.c
+    with selfdiffphi, fNL = 0) on a noise spectrum: (vel, off), each (3, n^3)
+    float32 in lattice order z, y, x."""
+    d = np.ascontiguousarray(den, np.complex64).view(np.float32).reshape(-1).copy()
+    vel = np.zeros((3, n ** 3), np.float32)
+    off = np.zeros((3, n ** 3), np.float32)
+    ref(VARIANT_A).ref_two_lpt(ctypes.c_int(n), d.ctypes.data_as(ctypes.c_void_p), ctypes.c_float(amp1),
+                               ctypes.c_float(amp2), ctypes.c_float(vamp1), ctypes.c_float(vamp2),
+                               vel.ctypes.data_as(ctypes.c_void_p), off.ctypes.data_as(ctypes.c_void_p))
+    return vel, off

@@ -606,3 +606,40 @@ int ref_zeldovich(int n, float fnl, float gnl, float *den, float *fx, float *fy,
   free(b);
   return 0;
 }
+
+/* Second-order Lagrangian initial conditions for one rank (PORDER = 2):
+ * the reference's TwoLPT (Cosmos/CosmosIC/TwoLPT.c:259-535, fNL = gNL = 0)
+ * on the noise spectrum den1, then per axis the combination amp1*phi1 +
+ * amp2*phi2 and the reference's selfdiffphi (TwoLPT.c:17-157), as
+ * TwoLPT_GetVR does (Cosmos/CosmosIC/cosmosic.h:141-163): velocities with
+ * (vamp1, vamp2) and offsets with (amp1, amp2). vel, off: 3 fields of n^3
+ * floats each, [z][y][x]. */
+void mpi_fftw_finalize(void) {}
+void TwoLPT(SimParameters *, DenType *, DenType *, DenType *, DenType *);
+void selfdiffphi(SimParameters *, DenType *, enum dimension);
+int ref_two_lpt(int n, const float *den1, float amp1, float amp2, float vamp1, float vamp2, float *vel, float *off) {
+  RefBox *b = refbox_new(n, 0.9f, 0.05f, 0.3f, 4.0f);
+  SimParameters *s = &b->sim;
+  size_t sz = (size_t)n * n * 2 * (n / 2 + 1), n3 = (size_t)n * n * n;
+  float *d1 = (float *)calloc(sz, sizeof(float)), *d2 = (float *)calloc(sz, sizeof(float));
+  float *w1 = (float *)calloc(sz, sizeof(float)), *w2 = (float *)calloc(sz, sizeof(float));
+  float *dfr = (float *)calloc(sz, sizeof(float));
+  memcpy(d1, den1, sizeof(float) * sz);
+  TwoLPT(s, d1, w1, w2, d2);
+  for (int pass = 0; pass < 2; pass++) {
+    float a1 = pass ? amp1 : vamp1, a2 = pass ? amp2 : vamp2;
+    float *out = pass ? off : vel;
+    for (int ax = 0; ax < 3; ax++) {
+      for (size_t i = 0; i < sz; i++) dfr[i] = a1 * d1[i] + a2 * d2[i];
+      selfdiffphi(s, dfr, (enum dimension)(ax + 1));
+      memcpy(out + ax * n3, dfr, sizeof(float) * n3);
+    }
+  }
+  free(d1);
+  free(d2);
+  free(w1);
+  free(w2);
+  free(dfr);
+  free(b);
+  return 0;
+}

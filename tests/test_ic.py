@@ -200,3 +200,32 @@ def test_ic_power_spectrum_follows_the_table():
     ratio = r["pk"][bins] * L ** 3 / want
     assert np.all((ratio > 0.8) & (ratio < 1.25)), ratio
     assert abs(float(np.mean(ratio)) - 1.0) < 0.1, ratio
+
+
+@pytest.mark.gpu
+@need_ref
+@pytest.mark.parametrize("n,seed", [(32, -11), (48, -5), (16, 2)])
+def test_engine_2lpt_matches_reference(n, seed):
+    """Second order against the reference's TwoLPT and selfdiffphi: the
+    velocities and offsets of the combined first- and second-order
+    potentials, within 1e-4 of their largest magnitude."""
+    vp = power_law_velpot(n) if seed < 0 else None
+    vamp, vamp2, damp1, damp2, pfact = 0.83, -0.61, 1.0, -3.0 / 7.0, float(n)
+    rec = E.ic_2lpt(n, seed, vp, vamp=vamp, vamp2=vamp2, damp1=damp1, damp2=damp2, pfact=pfact)
+    f32 = np.float32
+    vel, off = O.ref_two_lpt(n, O.ref_ic_noise(n, seed, vp), f32(pfact) * f32(damp1), f32(pfact) * f32(damp2),
+                             vamp, vamp2)
+    assert np.array_equal(rec["indx"], np.arange(n ** 3, dtype=np.uint64))
+    for a, c in enumerate("xyz"):
+        for got, want in ((rec["v" + c], vel[a]), (rec[c], off[a])):
+            scale = float(np.max(np.abs(want)))
+            assert scale > 0
+            assert np.max(np.abs(got - want)) <= 1e-4 * scale, c
+
+
+@pytest.mark.gpu
+def test_2lpt_rejects_non_gaussian_terms():
+    p = E.TpmIcParams()
+    p.n, p.iseed, p.fnl = 16, 3, 10.0
+    rec = np.empty(16 ** 3, E.DM_DTYPE)
+    assert E.load_library().tpm_ic_2lpt(p, rec.ctypes.data, E.MEM_HOST) == -1  # TPM_E_ARG
