@@ -335,14 +335,14 @@ TPM_D void dft_small<5>(float2 *v, float dir) {
 }
 
 template <int R>
-TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L, int Ns, int P,
+TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L, int ld, int Ns, int P,
                           float dir, int tid, int nth) {
   int jobs_per = L / R;
   int step = L / (Ns * R);
   for (int job = tid; job < P * jobs_per; job += nth) {
     int p = job / jobs_per, j = job - p * jobs_per;
-    const float2 *src = in + p * L;
-    float2 *dst = out + p * L;
+    const float2 *src = in + p * ld;
+    float2 *dst = out + p * ld;
     int k = j % Ns;
     float2 v[R];
 #pragma unroll
@@ -362,10 +362,10 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
   }
 }
 
-// Transforms P pencils of length L from a to scratch b and back as needed;
-// returns the buffer holding the result. dir = -1 forward, +1 backward
-// (unnormalised, FFTW sign convention).
-__device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, int P, float dir,
+// Transforms P pencils of length L (pencil p at p * ld) from a to scratch b
+// and back as needed; returns the buffer holding the result. dir = -1
+// forward, +1 backward (unnormalised, FFTW sign convention).
+__device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, int ld, int P, float dir,
                                const int *radix, int nf) {
   int tid = threadIdx.x, nth = blockDim.x;
   int Ns = 1;
@@ -373,13 +373,13 @@ __device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, in
   for (int s = 0; s < nf; s++) {
     int R = radix[s];
     if (R == 4)
-      stockham_stage<4>(in, out, tw, L, Ns, P, dir, tid, nth);
+      stockham_stage<4>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
     else if (R == 2)
-      stockham_stage<2>(in, out, tw, L, Ns, P, dir, tid, nth);
+      stockham_stage<2>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
     else if (R == 3)
-      stockham_stage<3>(in, out, tw, L, Ns, P, dir, tid, nth);
+      stockham_stage<3>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
     else
-      stockham_stage<5>(in, out, tw, L, Ns, P, dir, tid, nth);
+      stockham_stage<5>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
     __syncthreads();
     Ns *= R;
     float2 *t = in;
@@ -476,7 +476,7 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
     A[e] = v;
   }
   __syncthreads();
-  float2 *res = fft_pencils(A, B, twl, L, P, -1.f, a.radix, a.nf);
+  float2 *res = fft_pencils(A, B, twl, L, L, P, -1.f, a.radix, a.nf);
   for (int e = tid; e < P * hx; e += nth) {
     int p = e / hx, k = e - p * hx;
     int64_t row = row0 + p;
@@ -577,10 +577,12 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
                            const float2 *__restrict__ tw_n, int axis, float dir, int with_green, GreenArgs ga,
                            int TX, int nspec) {
   extern __shared__ float2 sm[];
-  int n = a.n, hx = a.hx, L = n, P = TX * nspec;
+  // pencils one element apart beyond their length: the transposing loads
+  // and stores (consecutive threads on consecutive pencils) hit distinct banks
+  int n = a.n, hx = a.hx, L = n, P = TX * nspec, Lp = n + 1;
   float2 *twl = sm;
   float2 *A = sm + L;
-  float2 *B = A + P * L;
+  float2 *B = A + P * Lp;
   int tid = threadIdx.x, nth = blockDim.x;
   for (int k = tid; k < L; k += nth) twl[k] = tw_n[k];
   int ntx = (hx + TX - 1) / TX;
@@ -595,18 +597,18 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     const float2 *src = q < TX ? spec : spec2;
     float2 v = make_float2(0.f, 0.f);
     if (qs < tw_) v = src[base + m * stride + kx0 + qs];
-    A[q * L + m] = v;
+    A[q * Lp + m] = v;
   }
   __syncthreads();
-  float2 *res = fft_pencils(A, B, twl, L, P, dir, a.radix, a.nf);
+  float2 *res = fft_pencils(A, B, twl, L, Lp, P, dir, a.radix, a.nf);
   if (with_green && ga.pk) {
-    float *sbin = reinterpret_cast<float *>(B + P * L);
+    float *sbin = reinterpret_cast<float *>(B + P * Lp);
     for (int e = tid; e < 2 * (n + 1); e += nth) sbin[e] = 0.f;
     __syncthreads();
     int wy = outer > n / 2 ? outer - n : outer;
     for (int e = tid; e < TX * L; e += nth) {
       int q = e / L, m = e - q * L;
-      if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[e]);
+      if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[q * Lp + m]);
     }
     __syncthreads();
     for (int e = tid; e < 2 * (n + 1); e += nth)
@@ -617,8 +619,8 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
       for (int e = tid; e < P * L; e += nth) {
         int q = e / L, m = e - q * L;
         float gk = green(ga, kx0 + q, outer, m);
-        float2 v = res[e];
-        res[e] = make_float2(v.x * gk, v.y * gk);
+        float2 v = res[q * Lp + m];
+        res[q * Lp + m] = make_float2(v.x * gk, v.y * gk);
       }
     } else {
       int wy = outer > n / 2 ? outer - n : outer;
@@ -629,23 +631,24 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
         if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
         float s, c;
         sincospif((float)(kx + wy + wz) / (float)n, &s, &c);
-        float2 r1 = res[e], r2 = res[e + TX * L];
+        int i1 = q * Lp + m, i2 = (q + TX) * Lp + m;
+        float2 r1 = res[i1], r2 = res[i2];
         // (rho1 + e^{i theta} rho2) / 2, then times G
         float2 rho = make_float2(0.5f * (r1.x + c * r2.x - s * r2.y), 0.5f * (r1.y + c * r2.y + s * r2.x));
         float2 ph = make_float2(rho.x * gk, rho.y * gk);
-        res[e] = ph;
-        res[e + TX * L] = make_float2(c * ph.x + s * ph.y, c * ph.y - s * ph.x);  // e^{-i theta} phi
+        res[i1] = ph;
+        res[i2] = make_float2(c * ph.x + s * ph.y, c * ph.y - s * ph.x);  // e^{-i theta} phi
       }
     }
     __syncthreads();
     float2 *other = res == A ? B : A;
-    res = fft_pencils(res, other, twl, L, P, 1.f, a.radix, a.nf);
+    res = fft_pencils(res, other, twl, L, Lp, P, 1.f, a.radix, a.nf);
   }
   for (int e = tid; e < P * L; e += nth) {
     int q = e % P, m = e / P;
     int qs = q % TX;
     float2 *dst = q < TX ? spec : spec2;
-    if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * L + m];
+    if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * Lp + m];
   }
 }
 
@@ -690,7 +693,7 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
     A[e] = Zk;
   }
   __syncthreads();
-  float2 *res = fft_pencils(A, B, twl, L, P, 1.f, a.radix, a.nf);
+  float2 *res = fft_pencils(A, B, twl, L, L, P, 1.f, a.radix, a.nf);
   for (int p = 0; p < P; p++) {
     int64_t row = row0 + p;
     if (row >= nrows) break;
@@ -738,7 +741,7 @@ static int pencils_for(int L, int want = 0) {
 static int cols_per_block(int n, int hx, int nspec, int want = 0) {
   int TX = want > 0 ? want : (n >= 256 ? 8 : 16);
   // room for the power-spectrum bins (2(n+1) floats) as well
-  int tmax = (int)(((160 * 1024 - 8 * (n + 1)) / (int)sizeof(float2) / n - 1) / (2 * nspec));
+  int tmax = (int)(((160 * 1024 - 8 * (n + 1)) / (int)sizeof(float2) - n) / (2 * nspec * (n + 1)));
   if (TX > tmax) TX = tmax;
   if (TX > hx) TX = hx;
   if (TX < 1) TX = 1;
@@ -825,7 +828,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   // columns
   int TX = cols_per_block(n, g.hx, nspec, want_tx);
   FftArgs ac = fft_args(n, n, TX * nspec);
-  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * n) + (pk ? sizeof(float) * 2 * (n + 1) : 0);
+  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * (n + 1)) + (pk ? sizeof(float) * 2 * (n + 1) : 0);
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   ga.law = law;
@@ -861,7 +864,7 @@ void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 
                                                                    p.tw, nrows);
   int TX = cols_per_block(n, g.hx, 1);
   FftArgs ac = fft_args(n, n, TX);
-  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   memset(&ga, 0, sizeof(ga));
@@ -879,7 +882,7 @@ void fft_inverse(const MeshGeom &g, const FftPlan &p, float2 *spec, float *phi_p
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
   int TX = cols_per_block(n, g.hx, 1);
   FftArgs ac = fft_args(n, n, TX);
-  size_t smc = sizeof(float2) * (n + 2 * TX * n);
+  size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   memset(&ga, 0, sizeof(ga));
