@@ -246,7 +246,7 @@ void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t 
 }
 
 // ------------------------------------------------------------------ FFT
-// Stockham autosort radix-4/2/3/5 transform of a batch of pencils held in
+// Stockham autosort radix-16/8/4/2/3/5 transform of a batch of pencils held in
 // shared memory (the formulation of Govindaraju et al., SC08): in stage s
 // with radix R and Ns = product of the earlier radices, job j reads
 // in[j + r L/R], twiddles by exp(dir 2 pi i r (j mod Ns) / (Ns R)), does a
@@ -260,6 +260,14 @@ struct Factors {
 static Factors factorize(int L) {
   Factors f;
   f.nf = 0;
+  while (L % 16 == 0) {
+    f.r[f.nf++] = 16;
+    L /= 16;
+  }
+  if (L % 8 == 0) {
+    f.r[f.nf++] = 8;
+    L /= 8;
+  }
   while (L % 4 == 0) {
     f.r[f.nf++] = 4;
     L /= 4;
@@ -334,6 +342,61 @@ TPM_D void dft_small<5>(float2 *v, float dir) {
   v[3] = csub(m2, n2);
 }
 
+// 8 points: even and odd halves by radix 4, combined with W8^k.
+template <>
+TPM_D void dft_small<8>(float2 *v, float dir) {
+  const float h = 0.70710678118654752440f;  // cos(pi/4)
+  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+  dft_small<4>(e, dir);
+  dft_small<4>(o, dir);
+  // W8^k = exp(dir 2 pi i k / 8)
+  float2 t1 = make_float2(h * (o[1].x - dir * o[1].y), h * (o[1].y + dir * o[1].x));
+  float2 t2 = cmuli(o[2], dir);
+  float2 t3 = make_float2(-h * (o[3].x + dir * o[3].y), h * (dir * o[3].x - o[3].y));
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], t1);
+  v[5] = csub(e[1], t1);
+  v[2] = cadd(e[2], t2);
+  v[6] = csub(e[2], t2);
+  v[3] = cadd(e[3], t3);
+  v[7] = csub(e[3], t3);
+}
+
+// 16 points as 4 x 4: transforms over n1 of v[4 n1 + n2], twiddles
+// W16^(n2 k1), transforms over n2; X[k1 + 4 k2].
+template <>
+TPM_D void dft_small<16>(float2 *v, float dir) {
+  const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;  // cos, sin of pi/8
+  const float h = 0.70710678118654752440f;
+  float2 y[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+    float2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+    dft_small<4>(t, dir);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) y[n2][k1] = t[k1];
+  }
+  // W16^m = (cos(m pi/8), dir sin(m pi/8)) for m = n2 k1 in {1, 2, 3, 4, 6, 9}
+  const float cw[10] = {1.f, c1, h, s1, 0.f, -s1, -h, -c1, -1.f, -c1};
+  const float sw[10] = {0.f, s1, h, c1, 1.f, c1, h, s1, 0.f, -s1};
+#pragma unroll
+  for (int n2 = 1; n2 < 4; n2++)
+#pragma unroll
+    for (int k1 = 1; k1 < 4; k1++) {
+      int m = n2 * k1;
+      float2 w = make_float2(cw[m], dir * sw[m]);
+      y[n2][k1] = cmul(y[n2][k1], w);
+    }
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    float2 t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+    dft_small<4>(t, dir);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
+  }
+}
+
 template <int R>
 TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L, int ld, int Ns, int P,
                           float dir, int tid, int nth) {
@@ -349,7 +412,7 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
     for (int r = 0; r < R; r++) {
       float2 x = src[j + r * jobs_per];
       if (r) {
-        float2 w = tw[(r * k * step) % L];
+        float2 w = tw[r * k * step];  // r k step < L: r < R, k < Ns, step = L / (Ns R)
         if (dir > 0) w.y = -w.y;
         x = cmul(x, w);
       }
@@ -372,7 +435,11 @@ __device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, in
   float2 *in = a, *out = b;
   for (int s = 0; s < nf; s++) {
     int R = radix[s];
-    if (R == 4)
+    if (R == 16)
+      stockham_stage<16>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
+    else if (R == 8)
+      stockham_stage<8>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
+    else if (R == 4)
       stockham_stage<4>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
     else if (R == 2)
       stockham_stage<2>(in, out, tw, L, ld, Ns, P, dir, tid, nth);
