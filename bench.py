@@ -158,6 +158,30 @@ def _restore_stdout(saved):
     os.close(saved)
 
 
+def run_ic(E, ic, n, local):
+    """Zel'dovich and second-order initial conditions of n^3 particles with a
+    CAMB-like spectrum (sigma_8 = 0.8, 500 Mpc/h box, growth 1/50): noise,
+    transforms and records in device memory; each call returns when its work
+    is done, so it is timed by the host clock around the call (best of 3)."""
+    import torch
+    k = np.exp(np.linspace(np.log(1e-3), np.log(50), 400))
+    p = 2e4 * (k / 0.02) / (1 + (k / 0.02) ** 3)
+    vp = ic.velpot_table(n, 500.0, k, p, growth=1.0 / 50, sigma8=0.8)
+    out = torch.empty(n ** 3 * E.DM_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
+    res = {"workload": f"{n}^3 lattice, CAMB-like P(k) table, seed -7", "particles": n ** 3}
+    for name, fn in (("zeldovich", lambda: E.ic_zeldovich(n, -7, vp, out=out)),
+                     ("2lpt", lambda: E.ic_2lpt(n, -7, vp, vamp2=-0.6, out=out))):
+        fn()
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            ts.append(1e3 * (time.perf_counter() - t0))
+        res[name] = {"ms": min(ts), "Mparticles/s": n ** 3 / (min(ts) * 1e-3) / 1e6}
+    return res
+
+
 def cpu_baseline():
     ps = reference_sample()
     saved = _quiet_stdout()
@@ -168,7 +192,24 @@ def cpu_baseline():
     return {"value": ps.np / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
             "sample": f"clustered workload at 128^3 ({ps.np} particles, 25 Plummer spheres), one "
                       f"pmmain + treecorrection of the reference built from its sources (variant A), "
-                      f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s"}
+                      f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s",
+            "ic_reference": reference_ic_time(128)}
+
+
+def reference_ic_time(n):
+    """The reference's Zel'dovich initial conditions at n^3 on the host: its
+    gasdev/ran3 mode loop and its Zeldovich (FFTs through the oracle's double
+    DFT in place of FFTW, which is not built)."""
+    from oracle import oracle as O
+    k2 = np.arange((n // 2) ** 2 + 1, dtype=np.float64)
+    rk = 2 * np.pi * np.sqrt(np.maximum(k2, 1.0))
+    vp = (0.05 * rk ** -1.0 / rk ** 2 * n ** 3).astype(np.float32)
+    t0 = time.perf_counter()
+    d = O.ref_ic_noise(n, -7, vp)
+    t1 = time.perf_counter()
+    O.ref_zeldovich(n, d)
+    t2 = time.perf_counter()
+    return {"particles": n ** 3, "noise_s": t1 - t0, "zeldovich_s": t2 - t1, "threads": 1}
 
 
 def run_reference_arm(args):
@@ -608,6 +649,8 @@ def run_engine_arm(args):
         ek = np.linalg.norm(fk[tg].astype(np.float64) - fe, axis=1) / np.linalg.norm(fe, axis=1)
         line["kdk"]["err_vs_ewald"] = {"rms": float(np.sqrt(np.mean(ek * ek))), "p99": float(np.percentile(ek, 99))}
     eng.close()
+    if not args.no_ic:
+        line["ic"] = run_ic(E, ic, n, local)
     box_law = REFERENCE_LAW if args.law == "reference" else BOX_LAW
     if not args.no_batched:
         line["ensemble"] = {"law": box_law, **run_batched(args, E, ic, box_law, local, dist)}
@@ -637,6 +680,7 @@ def main():
     ap.add_argument("--no-reference-law", action="store_true")
     ap.add_argument("--no-ewald", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ic", action="store_true", help="skip the initial-conditions block")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-box ensemble block")
     ap.add_argument("--no-served", action="store_true", help="skip the served request-loop block")
     ap.add_argument("--ensemble-boxes", type=int, default=64)

@@ -650,11 +650,19 @@ def ic_zeldovich(n: int, iseed: int, velpot=None, fnl: float = 0.0, gnl: float =
 
 
 def ic_2lpt(n: int, iseed: int, velpot=None, vamp: float = 1.0, vamp2: float = 0.0, damp1: float = 1.0,
-            damp2: float = -3.0 / 7.0, pfact: float | None = None, device: int = 0) -> np.ndarray:
-    """Second-order Lagrangian particles (tpm_ic_2lpt): n^3 DM_DTYPE records."""
+            damp2: float = -3.0 / 7.0, pfact: float | None = None, device: int = 0, out=None):
+    """Second-order Lagrangian particles (tpm_ic_2lpt): n^3 DM_DTYPE records
+    (or into the device tensor `out`)."""
     lib = load_library()
     p, keep = _ic_params(n, iseed, velpot, 0.0, 0.0, vamp, float(n if pfact is None else pfact), device)
     p.vamp2, p.damp1, p.damp2 = vamp2, damp1, damp2
+    if out is not None:
+        if out.numel() * out.element_size() < n ** 3 * DM_DTYPE.itemsize:
+            raise ValueError("out is smaller than n^3 records")
+        ptr, mem = _ptr(out)
+        _check(lib.tpm_ic_2lpt(ctypes.byref(p), ptr, mem))
+        del keep
+        return out
     rec = np.empty(n ** 3, DM_DTYPE)
     _check(lib.tpm_ic_2lpt(ctypes.byref(p), rec.ctypes.data, MEM_HOST))
     del keep
