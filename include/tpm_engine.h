@@ -368,6 +368,25 @@ int tpm_read_mesh(tpm_ctx *ctx, int which, float *out);
 
 /* ---- allocation-free ordering ---- */
 
+/* ---- Streamed evaluations. A caller that evaluates one particle set after
+ * another from host memory (the reference's pmmain/treecorrection callers
+ * hand over host arrays every step) can overlap the host copies with the
+ * evaluations: tpm_stream_submit queues the copy of `pos` (np x 3 uint32
+ * fixed point, host; pinned memory lets the copy run asynchronously), the
+ * evaluation of `parts` and the copy of the forces into `forces` (np x 3
+ * float, host, caller order), and returns a ticket at once. The copy-in of
+ * one submission and the copy-out of another run during the evaluation in
+ * between. At most two submissions are in flight: the third call fails with
+ * TPM_E_STATE until the first is waited for. Neither buffer may be touched
+ * before tpm_stream_wait(ticket) returns; it reports the evaluation's errors.
+ * The particles loaded in the context (tpm_load_*) stay as they were, unless
+ * a larger np made the context grow its buffers (then load again before
+ * tpm_compute_forces); tpm_read_forces has nothing to read afterwards. No
+ * counterpart in the reference, which evaluates synchronously. */
+int tpm_stream_submit(tpm_ctx *ctx, int64_t np, const uint32_t *pos, float *forces, unsigned parts,
+                      int64_t *ticket);
+int tpm_stream_wait(tpm_ctx *ctx, int64_t ticket);
+
 /* ---- Zel'dovich initial conditions (Cosmos/CosmosIC: PMSeedForce.c,
  * Zeldovich.c, MakeParticle.c). One particle per point of an n^3 lattice,
  * from the reference's random sequence (Numerical Recipes ran3/gasdev,

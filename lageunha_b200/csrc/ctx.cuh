@@ -43,6 +43,19 @@ struct tpm_ctx {
   cudaStream_t st_pm = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool overlapped = false;  // the last timed evaluation ran the two chains side by side
+  // streamed evaluations (tpm_stream_submit / tpm_stream_wait): two slots of
+  // positions and forces, a copy-in and a copy-out stream
+  struct {
+    cudaStream_t in = nullptr, out = nullptr;
+    uint32_t *pos[2] = {nullptr, nullptr};
+    float *force[2] = {nullptr, nullptr};
+    int64_t cap = 0;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    uint32_t *herr = nullptr;      // pinned, [2][8]: each slot's error flags
+    int64_t ticket[2] = {-1, -1};  // the submission a slot holds
+    bool pending[2] = {false, false};
+    int64_t next = 0;
+  } sp;
   // particles
   int64_t np = 0, cap = 0;
   uint32_t *pos = nullptr;
@@ -134,6 +147,13 @@ int launch_kick(tpm_ctx *c, cudaStream_t st, float f2pm, float f2tree, const dou
 int launch_drift(tpm_ctx *c, cudaStream_t st, double pfact, const double *fac);
 // k_finish into c->fout: the summed forces in the caller's particle order.
 int launch_finish(tpm_ctx *c, cudaStream_t st);
+// grows the particle buffers to np (frees the loaded particles if it must)
+int ensure_particles_for(tpm_ctx *c, int64_t np);
+// the same into `out` with the given parts
+int launch_finish_to(tpm_ctx *c, cudaStream_t st, unsigned parts, float *out);
+// releases the buffers, streams and events of the streamed evaluations
+// (tpm_stream_*), after waiting for them
+void free_stream_state(tpm_ctx *c);
 // Device bytes a context of this mesh and particle capacity allocates.
 int64_t ctx_bytes(int n_mesh, int64_t np);
 // Parameter validation of tpm_create / tpm_set_params (sets the error).

@@ -474,6 +474,14 @@ int tpm::launch_finish(tpm_ctx *c, cudaStream_t st) {
   return 0;
 }
 
+int tpm::ensure_particles_for(tpm_ctx *c, int64_t np) { return ensure_particles(c, np); }
+
+int tpm::launch_finish_to(tpm_ctx *c, cudaStream_t st, unsigned parts, float *out) {
+  k_finish<<<grid_for(c->np), 256, 0, st>>>(c->perm, c->np, c->fpm, c->ftree, parts, out);
+  CK(cudaGetLastError());
+  return 0;
+}
+
 WalkBox tpm::ctx_walk_box(const tpm_ctx *c) {
   TreeParams tp;
   tp.n = (uint32_t)c->g.n;
@@ -591,6 +599,7 @@ int tpm_destroy(tpm_ctx *c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
+  free_stream_state(c);
   free_particles(c);
   free_mesh(c);
   if (c->law.tlog) cudaFree(c->law.tlog);

@@ -167,6 +167,8 @@ _SIGS = {
                                         ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
     "tpm_hubble_drag": (ctypes.c_int, [_P, ctypes.c_float]),
     "tpm_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float, ctypes.c_int32]),
+    "tpm_stream_submit": (ctypes.c_int, [_P, _I64, _P, _P, ctypes.c_uint, ctypes.POINTER(ctypes.c_int64)]),
+    "tpm_stream_wait": (ctypes.c_int, [_P, _I64]),
     "tpm_ic_noise": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
     "tpm_ic_zeldovich": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
     "tpm_ic_2lpt": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
@@ -387,6 +389,22 @@ class Engine:
                                          ctypes.addressof(s8), ctypes.addressof(sl))
         _check(k if k < 0 else 0)
         return {"pk": pk[:k], "cor": cor[:k], "sigma8": s8.value, "slope": sl.value}
+
+    def stream_submit(self, pos_host, forces_host, parts: int = PART_ALL) -> int:
+        """Queue one evaluation of host positions with its copies overlapped
+        (tpm_stream_submit); returns its ticket. Keep both buffers untouched
+        until stream_wait(ticket)."""
+        pp, pm = _ptr(pos_host)
+        fp, fm = _ptr(forces_host)
+        if pm != MEM_HOST or fm != MEM_HOST:
+            raise ValueError("stream_submit takes host buffers")
+        n = pos_host.shape[0]
+        t = ctypes.c_int64()
+        _check(self._lib.tpm_stream_submit(self._ctx, n, pp, fp, parts, ctypes.byref(t)))
+        return t.value
+
+    def stream_wait(self, ticket: int):
+        _check(self._lib.tpm_stream_wait(self._ctx, ticket))
 
     def hubble_drag(self, fact1: float):
         _check(self._lib.tpm_hubble_drag(self._ctx, fact1))
