@@ -407,6 +407,9 @@ typedef struct tpm_ic_params {
   /* second order only (tpm_ic_2lpt): COS_VAMP2, COS_DAMP1, COS_DAMP2
      (PMSeedForce.c:250-305; damp1 = 1, damp2 = -3/7 in the reference) */
   float vamp2, damp1, damp2;
+  /* second order with fnl or gnl (TwoLPT.c:284-335): COSBOXSIZE [Mpc/h],
+     OMEP, AMAX and the growth factor COS_GROWTH = bini/bnow */
+  float boxsize, omep, amax, growth;
 } tpm_ic_params;
 
 /* The noise spectrum of PMSeedForce.c:293-399 (one rank): spec receives
@@ -426,10 +429,11 @@ int tpm_ic_zeldovich(const tpm_ic_params *p, void *records, int mem);
 
 /* Second-order Lagrangian particles (PORDER = 2): TwoLPTmain
  * (Cosmos/CosmosIC/TwoLPTmain.c:157-240) for one rank. The second-order
- * potential of TwoLPT (TwoLPT.c:259-535) from the same noise; velocity
- * d/dx (vamp phi1 + vamp2 phi2) and offset d/dx (pfact damp1 phi1 +
- * pfact damp2 phi2) per axis (TwoLPT_GetVR, cosmosic.h:141-163). Same
- * records as tpm_ic_zeldovich; fnl and gnl must be 0. */
+ * potential of TwoLPT (TwoLPT.c:259-535) from the same noise, after its
+ * non-Gaussian terms when fnl or gnl is set; velocity d/dx (vamp phi1 +
+ * vamp2 phi2) and offset d/dx (pfact damp1 phi1 + pfact damp2 phi2) per
+ * axis (TwoLPT_GetVR, cosmosic.h:141-163). Same records as
+ * tpm_ic_zeldovich. */
 int tpm_ic_2lpt(const tpm_ic_params *p, void *records, int mem);
 
 /* Largest particle count tpm_morton_order_noalloc accepts: its scratch is a

@@ -97,7 +97,8 @@ class TpmIcParams(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("n", ctypes.c_int32), ("iseed", ctypes.c_int64),
                 ("velpot", ctypes.c_void_p), ("fnl", ctypes.c_float), ("gnl", ctypes.c_float),
                 ("vamp", ctypes.c_float), ("pfact", ctypes.c_float), ("vamp2", ctypes.c_float),
-                ("damp1", ctypes.c_float), ("damp2", ctypes.c_float)]
+                ("damp1", ctypes.c_float), ("damp2", ctypes.c_float), ("boxsize", ctypes.c_float),
+                ("omep", ctypes.c_float), ("amax", ctypes.c_float), ("growth", ctypes.c_float)]
 
 
 class EngineError(RuntimeError):
@@ -668,12 +669,15 @@ def ic_zeldovich(n: int, iseed: int, velpot=None, fnl: float = 0.0, gnl: float =
 
 
 def ic_2lpt(n: int, iseed: int, velpot=None, vamp: float = 1.0, vamp2: float = 0.0, damp1: float = 1.0,
-            damp2: float = -3.0 / 7.0, pfact: float | None = None, device: int = 0, out=None):
+            damp2: float = -3.0 / 7.0, pfact: float | None = None, device: int = 0, out=None, fnl: float = 0.0,
+            gnl: float = 0.0, boxsize: float = 0.0, omep: float = 0.0, amax: float = 0.0, growth: float = 0.0):
     """Second-order Lagrangian particles (tpm_ic_2lpt): n^3 DM_DTYPE records
-    (or into the device tensor `out`)."""
+    (or into the device tensor `out`); fnl/gnl need boxsize, omep, amax and
+    growth (COS_GROWTH)."""
     lib = load_library()
-    p, keep = _ic_params(n, iseed, velpot, 0.0, 0.0, vamp, float(n if pfact is None else pfact), device)
+    p, keep = _ic_params(n, iseed, velpot, fnl, gnl, vamp, float(n if pfact is None else pfact), device)
     p.vamp2, p.damp1, p.damp2 = vamp2, damp1, damp2
+    p.boxsize, p.omep, p.amax, p.growth = boxsize, omep, amax, growth
     if out is not None:
         if out.numel() * out.element_size() < n ** 3 * DM_DTYPE.itemsize:
             raise ValueError("out is smaller than n^3 records")

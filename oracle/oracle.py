@@ -373,14 +373,16 @@ def ref_zeldovich(n, den, fnl=0.0, gnl=0.0):
     return tuple(a[:, :, :n] for a in f)
 
 
-def ref_two_lpt(n, den, amp1, amp2, vamp1, vamp2):
+def ref_two_lpt(n, den, amp1, amp2, vamp1, vamp2, fnl=0.0, gnl=0.0, boxsize=100.0, omep=0.3, amax=50.0,
+                growth=0.02):
     """The reference's second-order initial conditions for one rank (TwoLPT.c
-    with selfdiffphi, fNL = 0) on a noise spectrum: (vel, off), each (3, n^3)
-    float32 in lattice order z, y, x."""
+    with selfdiffphi) on a noise spectrum: (vel, off), each (3, n^3) float32
+    in lattice order z, y, x."""
     d = np.ascontiguousarray(den, np.complex64).view(np.float32).reshape(-1).copy()
     vel = np.zeros((3, n ** 3), np.float32)
     off = np.zeros((3, n ** 3), np.float32)
-    ref(VARIANT_A).ref_two_lpt(ctypes.c_int(n), d.ctypes.data_as(ctypes.c_void_p), ctypes.c_float(amp1),
-                               ctypes.c_float(amp2), ctypes.c_float(vamp1), ctypes.c_float(vamp2),
+    f = ctypes.c_float
+    ref(VARIANT_A).ref_two_lpt(ctypes.c_int(n), d.ctypes.data_as(ctypes.c_void_p), f(amp1), f(amp2), f(vamp1),
+                               f(vamp2), f(fnl), f(gnl), f(boxsize), f(omep), f(amax), f(growth),
                                vel.ctypes.data_as(ctypes.c_void_p), off.ctypes.data_as(ctypes.c_void_p))
     return vel, off

@@ -608,7 +608,8 @@ int ref_zeldovich(int n, float fnl, float gnl, float *den, float *fx, float *fy,
 }
 
 /* Second-order Lagrangian initial conditions for one rank (PORDER = 2):
- * the reference's TwoLPT (Cosmos/CosmosIC/TwoLPT.c:259-535, fNL = gNL = 0)
+ * the reference's TwoLPT (Cosmos/CosmosIC/TwoLPT.c:259-535, its fNL/gNL
+ * branch with the box size, Omega_m, amax and growth factor given)
  * on the noise spectrum den1, then per axis the combination amp1*phi1 +
  * amp2*phi2 and the reference's selfdiffphi (TwoLPT.c:17-157), as
  * TwoLPT_GetVR does (Cosmos/CosmosIC/cosmosic.h:141-163): velocities with
@@ -617,9 +618,16 @@ int ref_zeldovich(int n, float fnl, float gnl, float *den, float *fx, float *fy,
 void mpi_fftw_finalize(void) {}
 void TwoLPT(SimParameters *, DenType *, DenType *, DenType *, DenType *);
 void selfdiffphi(SimParameters *, DenType *, enum dimension);
-int ref_two_lpt(int n, const float *den1, float amp1, float amp2, float vamp1, float vamp2, float *vel, float *off) {
+int ref_two_lpt(int n, const float *den1, float amp1, float amp2, float vamp1, float vamp2, float fnl, float gnl,
+                float boxsize, float omep, float amax, float growth, float *vel, float *off) {
   RefBox *b = refbox_new(n, 0.9f, 0.05f, 0.3f, 4.0f);
   SimParameters *s = &b->sim;
+  FNL(s) = fnl;
+  GNL(s) = gnl;
+  COSBOXSIZE(s) = boxsize;
+  OMEP(s) = omep;
+  AMAX(s) = amax;
+  COS_GROWTH(s) = growth;
   size_t sz = (size_t)n * n * 2 * (n / 2 + 1), n3 = (size_t)n * n * n;
   float *d1 = (float *)calloc(sz, sizeof(float)), *d2 = (float *)calloc(sz, sizeof(float));
   float *w1 = (float *)calloc(sz, sizeof(float)), *w2 = (float *)calloc(sz, sizeof(float));

@@ -224,7 +224,26 @@ def test_engine_2lpt_matches_reference(n, seed):
 
 
 @pytest.mark.gpu
-def test_2lpt_rejects_non_gaussian_terms():
+@need_ref
+@pytest.mark.parametrize("n,fnl,gnl", [(32, 100.0, 0.0), (24, 40.0, 2.0e4)])
+def test_engine_2lpt_non_gaussian_matches_reference(n, fnl, gnl):
+    """TwoLPT's non-Gaussian branch (TwoLPT.c:284-335: to the real potential,
+    the local terms with the growth corrections, and back)."""
+    seed, vp = -13, power_law_velpot(n)
+    cos = dict(boxsize=200.0, omep=0.3, amax=50.0, growth=0.02)
+    vamp, vamp2, damp1, damp2, pfact = 0.83, -0.61, 1.0, -3.0 / 7.0, float(n)
+    rec = E.ic_2lpt(n, seed, vp, vamp=vamp, vamp2=vamp2, damp1=damp1, damp2=damp2, pfact=pfact, fnl=fnl, gnl=gnl,
+                    **cos)
+    f32 = np.float32
+    vel, off = O.ref_two_lpt(n, O.ref_ic_noise(n, seed, vp), f32(pfact) * f32(damp1), f32(pfact) * f32(damp2),
+                             vamp, vamp2, fnl=fnl, gnl=gnl, **cos)
+    for a, c in enumerate("xyz"):
+        for got, want in ((rec["v" + c], vel[a]), (rec[c], off[a])):
+            assert np.max(np.abs(got - want)) <= 1e-4 * float(np.max(np.abs(want))), c
+
+
+@pytest.mark.gpu
+def test_2lpt_non_gaussian_needs_the_cosmology():
     p = E.TpmIcParams()
     p.n, p.iseed, p.fnl = 16, 3, 10.0
     rec = np.empty(16 ** 3, E.DM_DTYPE)
