@@ -107,10 +107,10 @@ def _noise_close(got, want):
 @pytest.mark.gpu
 @need_ref
 @pytest.mark.parametrize("n,seed,weighted", [(16, 3, False), (32, -11, True), (48, -5, True), (128, -2024, True),
-                                             (256, 7, False)])
+                                             (256, 7, False), (512, -99, True)])
 def test_engine_noise_matches_reference(n, seed, weighted):
     """Sizes from one chunk of the device's jump-ahead stream (16) to many
-    (128: 3 level-2 starts, 256: 23)."""
+    (128: 3 level-2 starts, 256: 23, 512: 177 starts over 45,312 chunks)."""
     vp = power_law_velpot(n) if weighted else None
     got = E.ic_noise(n, seed, vp)
     want = O.ref_ic_noise(n, seed, vp)
