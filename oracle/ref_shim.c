@@ -7,14 +7,19 @@
  * Compiled from the reference tree (not copied):
  *   Cosmos/pmmain.c, Cosmos/psolver.c, Cosmos/fda4.c, Cosmos/treecorrection.c,
  *   Cosmos/BasicCell.c, OST/ost.ver2.c, OST/Model4TreeForce.c,
- *   Timer/timerutil.c
+ *   Timer/timerutil.c, and for the step, snapshot, spectrum and initial
+ *   conditions Cosmos/CosmosEvolFactor.c, Cosmos/FLRW.c, Cosmos/mynr.c,
+ *   Cosmos/Correlation.c, Params/header.c, Cosmos/CosmosIC/nr.c,
+ *   Cosmos/CosmosIC/nrutil.c, Cosmos/CosmosIC/Zeldovich.c,
+ *   Cosmos/CosmosIC/TwoLPT.c
  * with -DINTEL -DXYZDBL -DGOTPM (sRules.make:32,46) and -fopenmp.
  *
  * What this file supplies for a single rank on one box:
  *  - MPI: the scalar Reduce/Bcast/Barrier calls of the force path become
  *    copies/no-ops (oracle/stub/mpi.h).
  *  - FFTW-MPI: fftwf_mpi_execute_dft_r2c / _c2r with the reference's plan
- *    flags FFTW_MPI_TRANSPOSED_OUT / _IN (FFT/fft.c:130-146): in-place,
+ *    flags FFTW_MPI_TRANSPOSED_OUT / _IN (FFT/fft.c:130-146), or without them
+ *    for the initial conditions' np/inp plans (FFT/fft.c:81-94): in-place,
  *    unnormalised, rows padded to 2*(nx/2+1) floats, spectrum stored as
  *    [y][z][x/2+1] (the layout psolver indexes, Cosmos/psolver.c:49-72).
  *    The arithmetic is oracle/dft.c in double. The vendored FFTW 3.3.6 is not
