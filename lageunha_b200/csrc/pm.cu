@@ -116,16 +116,14 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
     }
     return;
   }
-  // runs of equal home node: segmented sum onto the run's first lane
+  // runs of equal home node: segmented sum onto the run's first lane, in
+  // as many halving rounds as the warp's longest run needs
   unsigned le = heads & ((2u << lane) - 1u);
   int seg = 31 - __clz(le);
-  bool ok[5];
-#pragma unroll
-  for (int j = 0; j < 5; j++) {
-    int o = 1 << j;
-    int s2 = __shfl_down_sync(0xffffffffu, seg, o);
-    ok[j] = (lane + o < 32) && s2 == seg;
-  }
+  unsigned above = heads & ~((2u << lane) - 1u);
+  unsigned run = head ? (unsigned)((above ? __ffs(above) - 1 : 32) - lane) : 1u;
+  unsigned maxrun = __reduce_max_sync(0xffffffffu, run);
+  int rounds = 32 - __clz((int)maxrun - 1);
   float w[27];
 #pragma unroll
   for (int c = 0; c < 3; c++)
@@ -133,12 +131,14 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
     for (int b = 0; b < 3; b++)
 #pragma unroll
       for (int a = 0; a < 3; a++) w[a + 3 * b + 9 * c] = wx[a] * wy[b] * wz[c];
-#pragma unroll
-  for (int j = 0; j < 5; j++) {
+  for (int j = 0; j < rounds; j++) {
+    int o = 1 << j;
+    int s2 = __shfl_down_sync(0xffffffffu, seg, o);
+    bool ok = (lane + o < 32) && s2 == seg;
 #pragma unroll
     for (int q = 0; q < 27; q++) {
-      float y = __shfl_down_sync(0xffffffffu, w[q], 1 << j);
-      if (ok[j]) w[q] += y;
+      float y = __shfl_down_sync(0xffffffffu, w[q], o);
+      if (ok) w[q] += y;
     }
   }
   if (valid && head) {
@@ -257,14 +257,18 @@ struct Factors {
   int r[16];
 };
 
-static Factors factorize(int L) {
+// radices of the x passes (packed rows) and of the column passes
+constexpr int kXRadixMax = 16;
+constexpr int kColRadixMax = 16;
+
+static Factors factorize(int L, int rmax) {
   Factors f;
   f.nf = 0;
-  while (L % 16 == 0) {
+  while (rmax >= 16 && L % 16 == 0) {
     f.r[f.nf++] = 16;
     L /= 16;
   }
-  if (L % 8 == 0) {
+  if (rmax >= 8 && L % 8 == 0) {
     f.r[f.nf++] = 8;
     L /= 8;
   }
@@ -463,12 +467,12 @@ struct FftArgs {
   int P;              // pencils per block
 };
 
-static FftArgs fft_args(int n, int L, int P) {
+static FftArgs fft_args(int n, int L, int P, int rmax) {
   FftArgs a;
   a.n = n;
   a.hx = n / 2 + 1;
   a.L = L;
-  Factors f = factorize(L);
+  Factors f = factorize(L, rmax);
   a.nf = f.nf;
   for (int i = 0; i < 16; i++) a.radix[i] = i < f.nf ? f.r[i] : 1;
   a.P = P;
@@ -885,7 +889,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   bool packed = (n % 2) == 0;
   int Lx = packed ? n / 2 : n;
   int Px = pencils_for(Lx, want_px);
-  FftArgs ax = fft_args(n, Lx, Px);
+  FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
   const float2 *twL = packed ? p.tw_half : p.tw;
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
   int thx = 256;
@@ -894,7 +898,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   if (rho2) k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho2, spec2, ax, twL, p.tw, nrows);
   // columns
   int TX = cols_per_block(n, g.hx, nspec, want_tx);
-  FftArgs ac = fft_args(n, n, TX * nspec);
+  FftArgs ac = fft_args(n, n, TX * nspec, kColRadixMax);
   size_t smc = sizeof(float2) * (n + 2 * TX * nspec * (n + 1)) + (pk ? sizeof(float) * 2 * (n + 1) : 0);
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
@@ -925,12 +929,12 @@ void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 
   bool packed = (n % 2) == 0;
   int Lx = packed ? n / 2 : n;
   int Px = pencils_for(Lx);
-  FftArgs ax = fft_args(n, Lx, Px);
+  FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
   k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), 256, smx, st>>>(real, spec, ax, packed ? p.tw_half : p.tw,
                                                                    p.tw, nrows);
   int TX = cols_per_block(n, g.hx, 1);
-  FftArgs ac = fft_args(n, n, TX);
+  FftArgs ac = fft_args(n, n, TX, kColRadixMax);
   size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
@@ -945,10 +949,10 @@ void fft_inverse(const MeshGeom &g, const FftPlan &p, float2 *spec, float *phi_p
   bool packed = (n % 2) == 0;
   int Lx = packed ? n / 2 : n;
   int Px = pencils_for(Lx);
-  FftArgs ax = fft_args(n, Lx, Px);
+  FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
   size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
   int TX = cols_per_block(n, g.hx, 1);
-  FftArgs ac = fft_args(n, n, TX);
+  FftArgs ac = fft_args(n, n, TX, kColRadixMax);
   size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
