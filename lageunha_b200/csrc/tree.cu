@@ -507,9 +507,13 @@ struct WarpLists {
   WalkBox box;                     // the box of the group this warp walks
   uint32_t pc[kPcCap];
   uint32_t pp[kPpBatch];
-  float4 stage[kPpBatch];          // PP: one float4 per source; PC: three per node
+  float4 stage[kPpBatch];          // PP: x, y, z rows of the sources; PC: three float4 per node
   uint32_t stack[kStackSmem];
 };
+
+// the stage buffer holds the particle rows (x, y, z of kPpBatch sources, read
+// four past the last) and the node rows (11 of 32)
+static_assert(3 * kPpBatch + 4 <= 4 * kPpBatch && 11 * 32 <= 4 * kPpBatch, "stage buffer too small");
 
 struct WalkCtx {
   float tx, ty, tz;       // this lane's target relative to u_ref (cells)
@@ -519,34 +523,57 @@ struct WalkCtx {
   uint32_t rx, ry, rz;    // u_ref
 };
 
+// The law at s = r^2 + kLogR2Floor (cells^2) from the table indexed by the
+// float bits of s: the exponent and the top kLogMantissa mantissa bits pick
+// the bin, the remaining mantissa bits are the position inside it, so neither
+// a square root nor a conversion is needed, and s >= 2^-20 needs no lower
+// clamp. tlb is the table's shared address with the base entry kLogBase
+// folded in (s >= 2^-20 keeps the entry >= 0; the clamp keeps it in range).
+TPM_D float law_at(float s, uint32_t tlb) {
+  uint32_t bits = __float_as_uint(s);
+  uint32_t kk = min(bits >> kLogShift, (uint32_t)(kLogBase + kLogEntries));
+  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
+  float2 c;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
+  return fmaf(c.y, m, c.x);
+}
+
 // One source against this lane's target: the reference's AddPar
-// (OST/ost.ver2.c:279-293) without the mass factor. The law comes from the
-// table indexed by the float bits of s = r^2 + kLogR2Floor (cells^2): the
-// exponent and the top kLogMantissa mantissa bits pick the bin, the remaining
-// mantissa bits are the position inside it, so neither a square root nor a
-// conversion is needed, and s >= 2^-20 needs no lower clamp. The target
+// (OST/ost.ver2.c:279-293) without the mass factor. The source comes negated
+// (nsx = -x), so dx = tx + nsx is the IEEE difference tx - x. The target
 // itself (r = 0) lands in bin 0 with a zero separation, adding nothing.
 // kHardCut: the per-pair cut of the reference law, tested as s <= rsphere^2
 // (a cut 2^-20 cells^2 inside r^2 <= rsphere^2); the Gaussian law's table is
 // zero from the cut on and needs no test.
 template <bool kHardCut>
-TPM_D void pp_body(const float4 s, const WalkCtx &w, float rs2, const float2 *__restrict__ tl, float &ax,
-                   float &ay, float &az) {
-  float dx = w.tx - s.x, dy = w.ty - s.y, dz = w.tz - s.z;
+TPM_D void pp_one(float nsx, float nsy, float nsz, const WalkCtx &w, float rs2, uint32_t tlb, float &ax,
+                  float &ay, float &az) {
+  float dx = w.tx + nsx, dy = w.ty + nsy, dz = w.tz + nsz;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
-  uint32_t bits = __float_as_uint(r2);
-  // entry (bits >> kLogShift) - kLogBase, the base folded into the shared
-  // address (s >= 2^-20 keeps the entry >= 0; the clamp keeps it in range)
-  uint32_t kk = min(bits >> kLogShift, (uint32_t)(kLogBase + kLogEntries));
-  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
-  uint32_t tlb = (uint32_t)__cvta_generic_to_shared(tl) - (uint32_t)(kLogBase * 8);
-  float2 c;
-  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
-  float f = fmaf(c.y, m, c.x);
+  float f = law_at(r2, tlb);
   if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
   ay = fmaf(dy, f, ay);
   az = fmaf(dz, f, az);
+}
+
+// Two sources against this lane's target, the separations, r^2 and the
+// accumulation as packed fp32x2 operations (sm_100 add/fma on register
+// pairs): each half is the IEEE fp32 operation pp_one does, in the same
+// order, so the sums are the same bits as two pp_one calls into the halves.
+template <bool kHardCut>
+TPM_D void pp_two(float2 nsx, float2 nsy, float2 nsz, float2 tx, float2 ty, float2 tz, float rs2, uint32_t tlb,
+                  float2 &ax, float2 &ay, float2 &az) {
+  float2 dx = __fadd2_rn(tx, nsx), dy = __fadd2_rn(ty, nsy), dz = __fadd2_rn(tz, nsz);
+  float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(kLogR2Floor, kLogR2Floor))));
+  float2 f = make_float2(law_at(r2.x, tlb), law_at(r2.y, tlb));
+  if (kHardCut) {
+    f.x = r2.x <= rs2 ? f.x : 0.f;
+    f.y = r2.y <= rs2 ? f.y : 0.f;
+  }
+  ax = __ffma2_rn(dx, f, ax);
+  ay = __ffma2_rn(dy, f, ay);
+  az = __ffma2_rn(dz, f, az);
 }
 
 // The group's bounding box (cells, relative to u_ref) and the squared reach
@@ -559,13 +586,17 @@ struct GroupBox {
 
 // Particle sources of the batch wl.pp[0..m): each lane loads one source,
 // drops it if it lies beyond the group's reach (it would add nothing to any
-// lane), and the kept ones are compacted, in order, into wl.stage; then every
-// lane evaluates every kept source against its target.
+// lane), and the kept ones are compacted, in order and negated, into the
+// x, y and z rows of wl.stage; then every lane evaluates every kept source
+// against its target, four at a time (one 16-byte broadcast load per row,
+// two packed pairs), sources j, j+1, j+2, j+3 into accumulator sets 0-3.
 template <bool kHardCut>
 TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
                    const GroupBox &gb, float rs2, const float2 *__restrict__ tl, unsigned long long &npp) {
   int lane = threadIdx.x & 31;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
+  float *nsx = reinterpret_cast<float *>(wl.stage);
+  float *nsy = nsx + kPpBatch, *nsz = nsx + 2 * kPpBatch;
   // all loads of the batch are issued before any is used
   uint32_t u[kPpBatch / 32][3];
 #pragma unroll
@@ -594,25 +625,45 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
       keep = dx * dx + dy * dy + dz * dz <= gb.reach2;
     }
     unsigned mk = __ballot_sync(0xffffffffu, keep);
-    if (keep) wl.stage[kept + __popc(mk & lanemask_lt)] = make_float4(px, py, pz, 0.f);
+    if (keep) {
+      int at = kept + __popc(mk & lanemask_lt);
+      nsx[at] = -px;
+      nsy[at] = -py;
+      nsz[at] = -pz;
+    }
     kept += __popc(mk);
   }
   __syncwarp();
   m = kept;
-  float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
-  float a2x = 0.f, a2y = 0.f, a2z = 0.f, a3x = 0.f, a3y = 0.f, a3z = 0.f;
+  const uint32_t tlb = (uint32_t)__cvta_generic_to_shared(tl) - (uint32_t)(kLogBase * 8);
+  const float2 tx = make_float2(w.tx, w.tx), ty = make_float2(w.ty, w.ty), tz = make_float2(w.tz, w.tz);
+  float2 a01x = make_float2(0.f, 0.f), a01y = a01x, a01z = a01x, a23x = a01x, a23y = a01x, a23z = a01x;
+  // the rows of the next four sources are loaded before the arithmetic of
+  // these four; past the last source that reads unused values still inside
+  // wl.stage (the z row ends 128 floats before it does)
   int j = 0;
-  for (; j + 4 <= m; j += 4) {
-    pp_body<kHardCut>(wl.stage[j], w, rs2, tl, a0x, a0y, a0z);
-    pp_body<kHardCut>(wl.stage[j + 1], w, rs2, tl, a1x, a1y, a1z);
-    pp_body<kHardCut>(wl.stage[j + 2], w, rs2, tl, a2x, a2y, a2z);
-    pp_body<kHardCut>(wl.stage[j + 3], w, rs2, tl, a3x, a3y, a3z);
+  if (m >= 4) {
+    float4 x = *reinterpret_cast<const float4 *>(nsx);
+    float4 y = *reinterpret_cast<const float4 *>(nsy);
+    float4 z = *reinterpret_cast<const float4 *>(nsz);
+    for (; j + 4 <= m; j += 4) {
+      float4 xn = *reinterpret_cast<const float4 *>(nsx + j + 4);
+      float4 yn = *reinterpret_cast<const float4 *>(nsy + j + 4);
+      float4 zn = *reinterpret_cast<const float4 *>(nsz + j + 4);
+      pp_two<kHardCut>(make_float2(x.x, x.y), make_float2(y.x, y.y), make_float2(z.x, z.y), tx, ty, tz, rs2, tlb,
+                       a01x, a01y, a01z);
+      pp_two<kHardCut>(make_float2(x.z, x.w), make_float2(y.z, y.w), make_float2(z.z, z.w), tx, ty, tz, rs2, tlb,
+                       a23x, a23y, a23z);
+      x = xn;
+      y = yn;
+      z = zn;
+    }
   }
-  for (; j < m; j++) pp_body<kHardCut>(wl.stage[j], w, rs2, tl, a0x, a0y, a0z);
+  for (; j < m; j++) pp_one<kHardCut>(nsx[j], nsy[j], nsz[j], w, rs2, tlb, a01x.x, a01y.x, a01z.x);
   if (w.active) {
-    w.ax += (a0x + a1x) + (a2x + a3x);
-    w.ay += (a0y + a1y) + (a2y + a3y);
-    w.az += (a0z + a1z) + (a2z + a3z);
+    w.ax += (a01x.x + a01x.y) + (a23x.x + a23x.y);
+    w.ay += (a01y.x + a01y.y) + (a23y.x + a23y.y);
+    w.az += (a01z.x + a01z.y) + (a23z.x + a23z.y);
     npp += (unsigned long long)m;
   }
   __syncwarp();
@@ -620,53 +671,72 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
 
 // Node terms: the reference's AddNode (OST/ost.ver2.c:247-277) with the y
 // and z components on their own axes. Coordinates are in cells; the log-r^2
-// tables in shared memory give the law and its derivatives.
+// tables in shared memory give the law and its derivatives. The batch's nodes
+// are staged as eleven rows of 32 (negated x, y, z, mass, Qxx, Qyy, Qzz, Qxy,
+// Qxz, Qyz, trQ; zero past the last node, which adds nothing) and evaluated
+// two at a time in packed fp32x2 operations; the quadrupole contraction is
+// d.(Qd) from the three rows of Qd.
 TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, float cpu, float rs2,
                    const float2 *__restrict__ tl, const float4 *__restrict__ tq, unsigned long long &npc) {
   int lane = threadIdx.x & 31;
+  float *row = reinterpret_cast<float *>(wl.stage);
+  const uint32_t tlb = (uint32_t)__cvta_generic_to_shared(tl) - (uint32_t)(kLogBase * 8);
+  const float2 tx = make_float2(w.tx, w.tx), ty = make_float2(w.ty, w.ty), tz = make_float2(w.tz, w.tz);
+  const float2 floor2 = make_float2(kLogR2Floor, kLogR2Floor);
   for (int base = 0; base < m_all; base += 32) {
     int m = min(32, m_all - base);
+    float v[11];
+#pragma unroll
+    for (int r = 0; r < 11; r++) v[r] = 0.f;
     if (lane < m) {
       uint32_t nd = wl.pc[base + lane];
       float4 m0 = tb.mom0[nd], m1 = tb.mom1[nd], m2 = tb.mom2[nd];
-      wl.stage[3 * lane + 0] = make_float4(wrapf(__float_as_uint(m0.x), w.rx, cpu),
-                                           wrapf(__float_as_uint(m0.y), w.ry, cpu),
-                                           wrapf(__float_as_uint(m0.z), w.rz, cpu), m0.w);
-      wl.stage[3 * lane + 1] = m1;  // Qxx Qyy Qzz Qxy
-      wl.stage[3 * lane + 2] = m2;  // Qxz Qyz trQ mass
+      v[0] = -wrapf(__float_as_uint(m0.x), w.rx, cpu);
+      v[1] = -wrapf(__float_as_uint(m0.y), w.ry, cpu);
+      v[2] = -wrapf(__float_as_uint(m0.z), w.rz, cpu);
+      v[3] = m0.w;                                      // mass
+      v[4] = m1.x, v[5] = m1.y, v[6] = m1.z, v[7] = m1.w;  // Qxx Qyy Qzz Qxy
+      v[8] = m2.x, v[9] = m2.y, v[10] = m2.z;             // Qxz Qyz trQ
     }
+#pragma unroll
+    for (int r = 0; r < 11; r++) row[32 * r + lane] = v[r];
     __syncwarp();
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    for (int j = 0; j < m; j++) {
-      float4 c0 = wl.stage[3 * j], q1 = wl.stage[3 * j + 1], q2 = wl.stage[3 * j + 2];
-      float dx = w.tx - c0.x, dy = w.ty - c0.y, dz = w.tz - c0.z;
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
+    for (int j = 0; j < m; j += 2) {
+      auto at = [&](int r) { return *reinterpret_cast<const float2 *>(row + 32 * r + j); };
+      float2 dx = __fadd2_rn(tx, at(0)), dy = __fadd2_rn(ty, at(1)), dz = __fadd2_rn(tz, at(2));
+      float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, floor2)));
       // f1 from the particle-particle table, f2 and f3 from the coarse one,
       // both indexed by the bits of r^2 (shared memory)
-      uint32_t bits = __float_as_uint(r2);
-      int k1 = min((int)(bits >> kLogShift) - kLogBase, kLogEntries);
-      float m1 = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
-      int k2 = min(max((int)(bits >> kPcShift) - kPcBase, 0), kPcEntries);
-      float m2 = __uint_as_float((bits & ((1u << kPcShift) - 1u)) | 0x3f800000u);
-      float2 c = tl[k1];
-      float4 d = tq[k2];
-      float f1 = fmaf(c.y, m1, c.x), f2 = fmaf(d.y, m2, d.x), f3 = fmaf(d.w, m2, d.z);
-      float Qxx = q1.x, Qyy = q1.y, Qzz = q1.z, Qxy = q1.w, Qxz = q2.x, Qyz = q2.y, trQ = q2.z;
-      float q1x = Qxx * dx + Qxy * dy + Qxz * dz;
-      float q2y = Qxy * dx + Qyy * dy + Qyz * dz;
-      float q3z = Qxz * dx + Qyz * dy + Qzz * dz;
-      float qq = Qxx * dx * dx + Qyy * dy * dy + Qzz * dz * dz + 2.f * (Qxy * dx * dy + Qxz * dx * dz + Qyz * dy * dz);
-      float tt = c0.w * f1 + trQ * f2 + qq * f3;
-      float two2 = 2.f * f2;
-      bool in = r2 <= rs2;
-      ax += in ? dx * tt + q1x * two2 : 0.f;
-      ay += in ? dy * tt + q2y * two2 : 0.f;
-      az += in ? dz * tt + q3z * two2 : 0.f;
+      float2 f1, f2, f3;
+      f1.x = law_at(r2.x, tlb);
+      f1.y = law_at(r2.y, tlb);
+      {
+        uint32_t b0 = __float_as_uint(r2.x), b1 = __float_as_uint(r2.y);
+        int k0 = min(max((int)(b0 >> kPcShift) - kPcBase, 0), kPcEntries);
+        int k1 = min(max((int)(b1 >> kPcShift) - kPcBase, 0), kPcEntries);
+        float m0 = __uint_as_float((b0 & ((1u << kPcShift) - 1u)) | 0x3f800000u);
+        float m1 = __uint_as_float((b1 & ((1u << kPcShift) - 1u)) | 0x3f800000u);
+        float4 d0 = tq[k0], d1 = tq[k1];
+        f2 = make_float2(fmaf(d0.y, m0, d0.x), fmaf(d1.y, m1, d1.x));
+        f3 = make_float2(fmaf(d0.w, m0, d0.z), fmaf(d1.w, m1, d1.z));
+      }
+      float2 qxx = at(4), qyy = at(5), qzz = at(6), qxy = at(7), qxz = at(8), qyz = at(9);
+      float2 q1x = __ffma2_rn(qxz, dz, __ffma2_rn(qxy, dy, __fmul2_rn(qxx, dx)));
+      float2 q2y = __ffma2_rn(qyz, dz, __ffma2_rn(qyy, dy, __fmul2_rn(qxy, dx)));
+      float2 q3z = __ffma2_rn(qzz, dz, __ffma2_rn(qyz, dy, __fmul2_rn(qxz, dx)));
+      float2 qq = __ffma2_rn(dz, q3z, __ffma2_rn(dy, q2y, __fmul2_rn(dx, q1x)));
+      float2 in = make_float2(r2.x <= rs2 ? 1.f : 0.f, r2.y <= rs2 ? 1.f : 0.f);
+      float2 tt = __fmul2_rn(__ffma2_rn(qq, f3, __ffma2_rn(at(10), f2, __fmul2_rn(at(3), f1))), in);
+      float2 two2 = __fmul2_rn(__fadd2_rn(f2, f2), in);
+      ax = __ffma2_rn(q1x, two2, __ffma2_rn(dx, tt, ax));
+      ay = __ffma2_rn(q2y, two2, __ffma2_rn(dy, tt, ay));
+      az = __ffma2_rn(q3z, two2, __ffma2_rn(dz, tt, az));
     }
     if (w.active) {
-      w.bx += ax;
-      w.by += ay;
-      w.bz += az;
+      w.bx += ax.x + ax.y;
+      w.by += ay.x + ay.y;
+      w.bz += az.x + az.y;
       npc += (unsigned long long)m;
     }
     __syncwarp();
@@ -825,14 +895,38 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
           }
         }
       }
-      // push children
+      // children to push (at most 8 per lane) and particles to append: one
+      // inclusive scan of both, packed as push | cnt << 9 (the push sum is at
+      // most 256 and the count sum below 2^23 while every count is below
+      // 2^18), else two scans
       uint32_t push = kind == 2 ? nch : 0u;
-      uint32_t incl = push;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
+      uint32_t cnt = kind == 3 ? pcnt : 0u;
+      uint32_t incl, pincl, total, ptotal;
+      if (__all_sync(0xffffffffu, cnt < (1u << 18))) {
+        uint32_t pk = push | (cnt << 9);
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t y = __shfl_up_sync(0xffffffffu, pk, o);
+          if (lane >= o) pk += y;
+        }
+        incl = pk & 511u;
+        pincl = pk >> 9;
+        uint32_t pkt = __shfl_sync(0xffffffffu, pk, 31);
+        total = pkt & 511u;
+        ptotal = pkt >> 9;
+      } else {
+        incl = push;
+        pincl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+          uint32_t y2 = __shfl_up_sync(0xffffffffu, pincl, o);
+          if (lane >= o) {
+            incl += y;
+            pincl += y2;
+          }
+        }
+        total = __shfl_sync(0xffffffffu, incl, 31);
+        ptotal = __shfl_sync(0xffffffffu, pincl, 31);
       }
-      uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
       if (top + (int)total > kStackCap) {
         failed = true;
         break;
@@ -857,13 +951,6 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
       // gives each lane its slice of the source list (lane order, as a
       // one-lane-at-a-time append would), flushed through eval_pp whenever
       // the batch fills
-      uint32_t cnt = kind == 3 ? pcnt : 0u;
-      uint32_t pincl = cnt;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, pincl, o);
-        if (lane >= o) pincl += y;
-      }
-      uint32_t ptotal = __shfl_sync(0xffffffffu, pincl, 31);
       uint32_t pexcl = pincl - cnt;
       uint32_t done = 0;
       while (done < ptotal) {
