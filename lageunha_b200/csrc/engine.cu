@@ -764,9 +764,8 @@ int tpm::enqueue_forces(tpm_ctx *c, unsigned parts, cudaStream_t st, bool timing
       launch_fda4(g, &c->tmap2, 2, c->spos, c->tile_start, c->fpm, c->err, pst);
       c->launches += 1;
     } else {
-      launch_fda4(g, &c->tmap4, 4, c->spos, c->tile_start, c->fpm, c->err, pst, 0, 0);
-      launch_fda4(g, &c->tmap4b, 4, c->spos, c->tile_start, c->fpm, c->err, pst, 1, 1);
-      c->launches += 2;
+      launch_fda4_pair(g, &c->tmap4, &c->tmap4b, c->spos, c->tile_start, c->fpm, c->err, pst);
+      c->launches += 1;
     }
     CK(stage_check(pst, "fda4"));
     if (timing) CK(cudaEventRecord(c->ev[4], pst));

@@ -94,6 +94,10 @@ void launch_green_opt(float *gt, int n, double rs, cudaStream_t st);
 void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const uint32_t *spos,
                  const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st, int half = 0,
                  int average = 0);
+// Both grids of the interlaced pair with the 8-point gradient in one pass:
+// fpm = the mean of the two grids' forces.
+void launch_fda4_pair(const MeshGeom &g, const CUtensorMap *tmap, const CUtensorMap *tmap2, const uint32_t *spos,
+                      const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st);
 // Tensor maps of the potential for the 4-point (radius 2) and the 8-point
 // (radius 4) gradient: their boxes differ.
 int make_phi_tensor_map(const MeshGeom &g, float *phi_pad, int radius, CUtensorMap *out);

@@ -257,6 +257,10 @@ struct Factors {
   int r[16];
 };
 
+// global loads each thread issues before it stores them into shared memory
+// (enough bytes in flight per SM for the transposing passes to stream)
+constexpr int kLoadBatch = 8;
+
 // radices of the x passes (packed rows) and of the column passes
 constexpr int kXRadixMax = 16;
 constexpr int kColRadixMax = 16;
@@ -533,18 +537,25 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
   for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
   int64_t row0 = (int64_t)blockIdx.x * P;
   bool packed = (L * 2 == n);
-  for (int e = tid; e < P * L; e += nth) {
-    int p = e / L, m = e - p * L;
-    int64_t row = row0 + p;
-    float2 v = make_float2(0.f, 0.f);
-    if (row < nrows) {
-      const float *r = rho + row * n;
-      if (packed)
-        v = *reinterpret_cast<const float2 *>(r + 2 * m);
-      else
-        v = make_float2(r[m], 0.f);
+  for (int e0 = tid; e0 < P * L; e0 += kLoadBatch * nth) {
+    float2 v[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; u++) {
+      int e = e0 + u * nth;
+      int p = e / L, m = e - p * L;
+      int64_t row = row0 + p;
+      v[u] = make_float2(0.f, 0.f);
+      if (e < P * L && row < nrows) {
+        const float *r = rho + row * n;
+        if (packed)
+          v[u] = *reinterpret_cast<const float2 *>(r + 2 * m);
+        else
+          v[u] = make_float2(r[m], 0.f);
+      }
     }
-    A[e] = v;
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; u++)
+      if (e0 + u * nth < P * L) A[e0 + u * nth] = v[u];
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, L, P, -1.f, a.radix, a.nf);
@@ -662,13 +673,22 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
   int64_t stride = axis == 1 ? (int64_t)hx : (int64_t)n * hx;
   int64_t base = axis == 1 ? (int64_t)outer * n * hx : (int64_t)outer * hx;
   int tw_ = min(TX, hx - kx0);
-  for (int e = tid; e < P * L; e += nth) {
-    int q = e % P, m = e / P;  // consecutive threads -> consecutive kx
-    int qs = q % TX;
-    const float2 *src = q < TX ? spec : spec2;
-    float2 v = make_float2(0.f, 0.f);
-    if (qs < tw_) v = src[base + m * stride + kx0 + qs];
-    A[q * Lp + m] = v;
+  for (int e0 = tid; e0 < P * L; e0 += kLoadBatch * nth) {
+    float2 v[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; u++) {
+      int e = e0 + u * nth;
+      int q = e % P, m = e / P;  // consecutive threads -> consecutive kx
+      int qs = q % TX;
+      const float2 *src = q < TX ? spec : spec2;
+      v[u] = make_float2(0.f, 0.f);
+      if (e < P * L && qs < tw_) v[u] = src[base + m * stride + kx0 + qs];
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; u++) {
+      int e = e0 + u * nth;
+      if (e < P * L) A[(e % P) * Lp + e / P] = v[u];
+    }
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, Lp, P, dir, a.radix, a.nf);
@@ -695,10 +715,23 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
       }
     } else {
       int wy = outer > n / 2 ? outer - n : outer;
-      for (int e = tid; e < TX * L; e += nth) {
+      for (int e0 = tid; e0 < TX * L; e0 += kLoadBatch * nth) {
+        float gks[kLoadBatch];
+        if (ga.gt) {
+#pragma unroll
+          for (int u = 0; u < kLoadBatch; u++) {
+            int e = e0 + u * nth;
+            int q = e / L, m = e - q * L;
+            gks[u] = e < TX * L && kx0 + q < hx ? ga.gt[((int64_t)outer * hx + kx0 + q) * n + m] : 0.f;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; u++) {
+        int e = e0 + u * nth;
+        if (e >= TX * L) break;
         int q = e / L, m = e - q * L;
         int kx = kx0 + q, wz = m > n / 2 ? m - n : m;
-        float gk = ga.gt ? ga.gt[((int64_t)outer * hx + kx) * n + m] : green(ga, kx, outer, m);
+        float gk = ga.gt ? gks[u] : green(ga, kx, outer, m);
         if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
         float s, c;
         sincospif((float)(kx + wy + wz) / (float)n, &s, &c);
@@ -709,6 +742,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
         float2 ph = make_float2(rho.x * gk, rho.y * gk);
         res[i1] = ph;
         res[i2] = make_float2(c * ph.x + s * ph.y, c * ph.y - s * ph.x);  // e^{-i theta} phi
+        }
       }
     }
     __syncthreads();
@@ -738,15 +772,34 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
   for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
   int64_t row0 = (int64_t)blockIdx.x * P;
   bool packed = (L * 2 == n);
-  for (int e = tid; e < P * L; e += nth) {
-    int p = e / L, k = e - p * L;
-    int64_t row = row0 + p;
-    float2 Zk = make_float2(0.f, 0.f);
-    if (row < nrows) {
-      const float2 *X = spec + row * hx;
+  constexpr int kB = kLoadBatch / 2;  // two loads per element
+  for (int e0 = tid; e0 < P * L; e0 += kB * nth) {
+    float2 xa[kB], xb[kB];
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      int e = e0 + u * nth;
+      int p = e / L, k = e - p * L;
+      int64_t row = row0 + p;
+      xa[u] = xb[u] = make_float2(0.f, 0.f);
+      if (e < P * L && row < nrows) {
+        const float2 *X = spec + row * hx;
+        if (packed) {
+          xa[u] = X[k];
+          xb[u] = X[L - k];
+        } else {
+          xa[u] = X[k < hx ? k : n - k];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kB; u++) {
+      int e = e0 + u * nth;
+      if (e >= P * L) break;
+      int k = e % L;
+      float2 Zk;
       if (packed) {
         // Z_k = (X_k + conj X_{L-k}) + i conj(W^k) (X_k - conj X_{L-k})
-        float2 xk = X[k], xc = cconj(X[L - k]);
+        float2 xk = xa[u], xc = cconj(xb[u]);
         if (k == 0) {
           xk.y = 0.f;
           xc.y = 0.f;
@@ -757,11 +810,11 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
         Zk = cadd(e2, make_float2(-t.y, t.x));
       } else {
         // full Hermitian row for odd n
-        Zk = k < hx ? X[k] : cconj(X[n - k]);
+        Zk = k < hx ? xa[u] : cconj(xa[u]);
         if (k == 0) Zk.y = 0.f;
       }
+      A[e] = Zk;
     }
-    A[e] = Zk;
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, L, P, 1.f, a.radix, a.nf);
@@ -1003,59 +1056,36 @@ TPM_D bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int64_t limit) {
   return false;
 }
 
+// One TMA load of the potential box around the tile (x from x0 - X0, 16-byte
+// aligned; y, z from -H) into box, completing the barrier's next phase; thread
+// 0 issues it. The box may hold the previous grid's potential: every thread
+// has passed a __syncthreads since its last read of it.
 template <int R>
-__global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CUtensorMap tmap,
-                                                      const uint32_t *__restrict__ spos,
-                                                      const uint32_t *__restrict__ tile_start, int n,
-                                                      int cbits, float *__restrict__ fpm,
-                                                      uint32_t *__restrict__ err, uint32_t half, int average) {
+TPM_D void fda_load_box(const CUtensorMap *tmap, float *box, uint64_t *bar, int x0, int y0, int z0) {
   using B = FdaBox<R>;
-  // dynamic shared memory: the potential box (128-byte aligned for TMA), then
-  // the gradient at the nodes as {-dphi/dx, -dphi/dy} pairs and -dphi/dz
-  extern __shared__ __align__(128) float fda_smem[];
-  float(*box)[B::BY][B::BX] = reinterpret_cast<float(*)[B::BY][B::BX]>(fda_smem);
-  float2 *gxy = reinterpret_cast<float2 *>(fda_smem + B::BY * B::BY * B::BX);
-  float *gz = reinterpret_cast<float *>(gxy + kGradSize);
-  __shared__ __align__(8) uint64_t bar;
-  int tid = threadIdx.x;
-  uint32_t t = blockIdx.x;
-  uint32_t tx = 0, ty = 0, tz = 0;
-  for (int b = 0; b < cbits - 3; b++) {
-    tx |= ((t >> (3 * b)) & 1u) << b;
-    ty |= ((t >> (3 * b + 1)) & 1u) << b;
-    tz |= ((t >> (3 * b + 2)) & 1u) << b;
-  }
-  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
-  if (p0 == p1) return;
-  int x0 = (int)tx * kTile, y0 = (int)ty * kTile, z0 = (int)tz * kTile;
-  if (tid == 0) {
-    uint32_t a = smem_u32(&bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t a = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    uint32_t a = smem_u32(bar);
     uint32_t bytes = sizeof(float) * B::BY * B::BY * B::BX;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
-    // box origin in padded coordinates: x from x0 - X0 (aligned), y,z from -H
     int cx = x0 - B::X0 + kGhost, cy = y0 - B::H + kGhost, cz = z0 - B::H + kGhost;
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(&box[0][0][0])),
-        "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(a)
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(box)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(cx), "r"(cy), "r"(cz), "r"(a)
         : "memory");
   }
-  if (!mbar_wait_bounded(&bar, 0, 1ll << 20)) {
-    if (tid == 0) atomicOr(err, (uint32_t)kErrTmaTimeout);
-    mbar_wait_bounded(&bar, 0, 1ll << 20);  // let an in-flight copy land before exit
-    return;
-  }
-  // gradient at nodes [t-1, t+T+1]^3, one line of kNodes nodes per thread
-  // and axis: the line's kNodes + 2R potential values are read once and the
-  // differences taken in registers
+}
+
+// -dphi/dx, -dphi/dy, -dphi/dz at the tile's nodes [t-1, t+T+1]^3, one line
+// of kNodes nodes per thread and axis: the line's kNodes + 2R potential
+// values are read once and the differences taken in registers.
+template <int R>
+TPM_D void fda_node_gradients(const float *boxf, float2 *gxy, float *gz) {
+  using B = FdaBox<R>;
+  const float(*box)[B::BY][B::BX] = reinterpret_cast<const float(*)[B::BY][B::BX]>(boxf);
   constexpr int kLine = kNodes + 2 * R;
-  for (int r = tid; r < 3 * kNodes * kNodes; r += kFdaThreads) {
+  for (int r = threadIdx.x; r < 3 * kNodes * kNodes; r += kFdaThreads) {
     int axis = r / (kNodes * kNodes), rr = r % (kNodes * kNodes);
     int p = rr % kNodes, q = rr / kNodes;
     // node (a, b, c) sits at box (a-1+X0, b-1+H, c-1+H); v[i] is the line's
@@ -1090,46 +1120,110 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
         gz[p + kGradSy * q + kGradSz * a] = f;
     }
   }
+}
+
+// The force at one particle: its 27 nodes' gradients with the TSC weights,
+// summed in the reference's order wt_n, n = a + 3b + 9c (fda4.h:67-102,
+// 276-292); node indices i1 = near, i2 = near + sign, i3 = near - sign
+// (fda4.h:46-54), relative to the tile's first node t - 1.
+TPM_D float3 fda_interp(const float2 *gxy, const float *gz, uint32_t ux, uint32_t uy, uint32_t uz, uint32_t n,
+                        uint32_t half, int x0, int y0, int z0) {
+  Axis ax = axis_of(ux, n, half), ay = axis_of(uy, n, half), az = axis_of(uz, n, half);
+  float wx1, wx2, wx3, wy1, wy2, wy3, wz1, wz2, wz3;
+  int sx, sy, sz;
+  tsc_w(ax.xmin, wx1, wx2, wx3, sx);
+  tsc_w(ay.xmin, wy1, wy2, wy3, sy);
+  tsc_w(az.xmin, wz1, wz2, wz3, sz);
+  int i1 = ax.near - (x0 - 1), j1 = ay.near - (y0 - 1), k1 = az.near - (z0 - 1);
+  int ii[3] = {i1, i1 + sx, i1 - sx}, jj[3] = {j1, j1 + sy, j1 - sy}, kk[3] = {k1, k1 + sz, k1 - sz};
+  float wxs[3] = {wx1, wx2, wx3}, wys[3] = {wy1, wy2, wy3}, wzs[3] = {wz1, wz2, wz3};
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      float wab[3] = {wxs[0] * wys[b], wxs[1] * wys[b], wxs[2] * wys[b]};
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        float wt = wab[a] * wzs[c];
+        int node = ii[a] + kGradSy * jj[b] + kGradSz * kk[c];
+        float2 g = gxy[node];
+        fx += wt * g.x;
+        fy += wt * g.y;
+        fz += wt * gz[node];
+      }
+    }
+  return make_float3(fx, fy, fz);
+}
+
+// kPair: both grids of the interlaced pair in one pass (tmap: the first grid,
+// particles as they are; tmap2: the second, particles moved by half a cell),
+// the force being the mean of the two; the box buffer is loaded twice and
+// both gradient sets kept. Else one grid (half as given), averaged with the
+// force already in fpm when average != 0.
+template <int R, bool kPair>
+__global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CUtensorMap tmap,
+                                                      const __grid_constant__ CUtensorMap tmap2,
+                                                      const uint32_t *__restrict__ spos,
+                                                      const uint32_t *__restrict__ tile_start, int n,
+                                                      int cbits, float *__restrict__ fpm,
+                                                      uint32_t *__restrict__ err, uint32_t half, int average) {
+  using B = FdaBox<R>;
+  // dynamic shared memory: the potential box (128-byte aligned for TMA), then
+  // the gradient at the nodes as {-dphi/dx, -dphi/dy} pairs and -dphi/dz
+  // (twice with kPair)
+  extern __shared__ __align__(128) float fda_smem[];
+  float *box = fda_smem;
+  float2 *gxy = reinterpret_cast<float2 *>(fda_smem + B::BY * B::BY * B::BX);
+  float *gz = reinterpret_cast<float *>(gxy + kGradSize);
+  float2 *gxy2 = reinterpret_cast<float2 *>(gz + kGradSize);
+  float *gz2 = reinterpret_cast<float *>(gxy2 + kGradSize);
+  __shared__ __align__(8) uint64_t bar;
+  int tid = threadIdx.x;
+  uint32_t t = blockIdx.x;
+  uint32_t tx = 0, ty = 0, tz = 0;
+  for (int b = 0; b < cbits - 3; b++) {
+    tx |= ((t >> (3 * b)) & 1u) << b;
+    ty |= ((t >> (3 * b + 1)) & 1u) << b;
+    tz |= ((t >> (3 * b + 2)) & 1u) << b;
+  }
+  uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
+  if (p0 == p1) return;
+  int x0 = (int)tx * kTile, y0 = (int)ty * kTile, z0 = (int)tz * kTile;
+  if (tid == 0) {
+    uint32_t a = smem_u32(&bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   __syncthreads();
+  constexpr int kGrids = kPair ? 2 : 1;
+#pragma unroll
+  for (int gi = 0; gi < kGrids; gi++) {
+    fda_load_box<R>(gi == 0 ? &tmap : &tmap2, box, &bar, x0, y0, z0);
+    if (!mbar_wait_bounded(&bar, (uint32_t)gi, 1ll << 20)) {
+      if (tid == 0) atomicOr(err, (uint32_t)kErrTmaTimeout);
+      mbar_wait_bounded(&bar, (uint32_t)gi, 1ll << 20);  // let an in-flight copy land before exit
+      return;
+    }
+    fda_node_gradients<R>(box, gi == 0 ? gxy : gxy2, gi == 0 ? gz : gz2);
+    __syncthreads();
+  }
   uint32_t nu = (uint32_t)n;
   for (uint32_t k = p0 + tid; k < p1; k += kFdaThreads) {
-    Axis ax = axis_of(spos[3 * (int64_t)k + 0], nu, half), ay = axis_of(spos[3 * (int64_t)k + 1], nu, half),
-         az = axis_of(spos[3 * (int64_t)k + 2], nu, half);
-    float wx1, wx2, wx3, wy1, wy2, wy3, wz1, wz2, wz3;
-    int sx, sy, sz;
-    tsc_w(ax.xmin, wx1, wx2, wx3, sx);
-    tsc_w(ay.xmin, wy1, wy2, wy3, sy);
-    tsc_w(az.xmin, wz1, wz2, wz3, sz);
-    // node indices i1 = near, i2 = near + sign, i3 = near - sign (fda4.h:46-54)
-    int i1 = ax.near - (x0 - 1), j1 = ay.near - (y0 - 1), k1 = az.near - (z0 - 1);
-    int ii[3] = {i1, i1 + sx, i1 - sx}, jj[3] = {j1, j1 + sy, j1 - sy}, kk[3] = {k1, k1 + sz, k1 - sz};
-    float wxs[3] = {wx1, wx2, wx3}, wys[3] = {wy1, wy2, wy3}, wzs[3] = {wz1, wz2, wz3};
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    // wt_n in the reference order n = a + 3b + 9c (fda4.h:67-102,276-292)
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-#pragma unroll
-      for (int b = 0; b < 3; b++) {
-        float wab[3] = {wxs[0] * wys[b], wxs[1] * wys[b], wxs[2] * wys[b]};
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          float wt = wab[a] * wzs[c];
-          int node = ii[a] + kGradSy * jj[b] + kGradSz * kk[c];
-          float2 g = gxy[node];
-          fx += wt * g.x;
-          fy += wt * g.y;
-          fz += wt * gz[node];
-        }
-      }
-    if (average) {
+    uint32_t ux = spos[3 * (int64_t)k + 0], uy = spos[3 * (int64_t)k + 1], uz = spos[3 * (int64_t)k + 2];
+    float3 f = fda_interp(gxy, gz, ux, uy, uz, nu, kPair ? 0u : half, x0, y0, z0);
+    if (kPair) {
+      // the mean of the two grids' forces
+      float3 f2 = fda_interp(gxy2, gz2, ux, uy, uz, nu, 1u, x0, y0, z0);
+      f = make_float3(0.5f * (f.x + f2.x), 0.5f * (f.y + f2.y), 0.5f * (f.z + f2.z));
+    } else if (average) {
       // the second grid of the interlaced pair: mean of the two grids' forces
-      fx = 0.5f * (fpm[3 * (int64_t)k + 0] + fx);
-      fy = 0.5f * (fpm[3 * (int64_t)k + 1] + fy);
-      fz = 0.5f * (fpm[3 * (int64_t)k + 2] + fz);
+      f = make_float3(0.5f * (fpm[3 * (int64_t)k + 0] + f.x), 0.5f * (fpm[3 * (int64_t)k + 1] + f.y),
+                      0.5f * (fpm[3 * (int64_t)k + 2] + f.z));
     }
-    fpm[3 * (int64_t)k + 0] = fx;
-    fpm[3 * (int64_t)k + 1] = fy;
-    fpm[3 * (int64_t)k + 2] = fz;
+    fpm[3 * (int64_t)k + 0] = f.x;
+    fpm[3 * (int64_t)k + 1] = f.y;
+    fpm[3 * (int64_t)k + 2] = f.z;
   }
 }
 
@@ -1171,15 +1265,23 @@ void launch_fda4(const MeshGeom &g, const CUtensorMap *tmap, int radius, const u
   const size_t nodes = sizeof(float) * 3 * kGradSize;
   if (radius == 2) {
     size_t smem = sizeof(float) * FdaBox<2>::BY * FdaBox<2>::BY * FdaBox<2>::BX + nodes;
-    cudaFuncSetAttribute(k_fda4<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fda4<2><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err,
-                                                 (uint32_t)half, average);
+    cudaFuncSetAttribute(k_fda4<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fda4<2, false><<<ntiles, kFdaThreads, smem, st>>>(*tmap, *tmap, spos, tile_start, g.n, g.cbits, fpm, err,
+                                                        (uint32_t)half, average);
   } else {
     size_t smem = sizeof(float) * FdaBox<4>::BY * FdaBox<4>::BY * FdaBox<4>::BX + nodes;
-    cudaFuncSetAttribute(k_fda4<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fda4<4><<<ntiles, kFdaThreads, smem, st>>>(*tmap, spos, tile_start, g.n, g.cbits, fpm, err,
-                                                 (uint32_t)half, average);
+    cudaFuncSetAttribute(k_fda4<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fda4<4, false><<<ntiles, kFdaThreads, smem, st>>>(*tmap, *tmap, spos, tile_start, g.n, g.cbits, fpm, err,
+                                                        (uint32_t)half, average);
   }
+}
+
+void launch_fda4_pair(const MeshGeom &g, const CUtensorMap *tmap, const CUtensorMap *tmap2, const uint32_t *spos,
+                      const uint32_t *tile_start, float *fpm, uint32_t *err, cudaStream_t st) {
+  uint32_t ntiles = 1u << (3 * (g.cbits - 3));
+  size_t smem = sizeof(float) * FdaBox<4>::BY * FdaBox<4>::BY * FdaBox<4>::BX + 2 * sizeof(float) * 3 * kGradSize;
+  cudaFuncSetAttribute(k_fda4<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_fda4<4, true><<<ntiles, kFdaThreads, smem, st>>>(*tmap, *tmap2, spos, tile_start, g.n, g.cbits, fpm, err, 0u, 0);
 }
 
 }  // namespace tpm
