@@ -212,15 +212,23 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
   __syncthreads();
   uint32_t nu = (uint32_t)n;
   int nwarp_items = (int)((p1 - p0 + 31) / 32) * 32;
+  // each thread's next particle is loaded before this one's deposit
+  uint32_t un[3] = {0u, 0u, 0u};
+  if ((uint32_t)tid < p1 - p0) {
+    int64_t i = (int64_t)p0 + tid;
+    un[0] = spos[3 * i + 0];
+    un[1] = spos[3 * i + 1];
+    un[2] = spos[3 * i + 2];
+  }
   for (int base = 0; base < nwarp_items; base += kDepThreads) {
     int k = base + tid;
     bool valid = (uint32_t)k < p1 - p0;
-    uint32_t u[3] = {0u, 0u, 0u};
-    if (valid) {
-      int64_t i = (int64_t)p0 + k;
-      u[0] = spos[3 * i + 0];
-      u[1] = spos[3 * i + 1];
-      u[2] = spos[3 * i + 2];
+    uint32_t u[3] = {un[0], un[1], un[2]};
+    if ((uint32_t)(k + kDepThreads) < p1 - p0) {
+      int64_t i = (int64_t)p0 + k + kDepThreads;
+      un[0] = spos[3 * i + 0];
+      un[1] = spos[3 * i + 1];
+      un[2] = spos[3 * i + 2];
     }
     float wx[3] = {0, 0, 0}, wy[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
     int home = 0;
@@ -1209,8 +1217,20 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
     __syncthreads();
   }
   uint32_t nu = (uint32_t)n;
+  // each thread's next particle is loaded before this one's interpolation
+  uint32_t ux = 0, uy = 0, uz = 0;
+  if (p0 + tid < p1) {
+    ux = spos[3 * (int64_t)(p0 + tid) + 0];
+    uy = spos[3 * (int64_t)(p0 + tid) + 1];
+    uz = spos[3 * (int64_t)(p0 + tid) + 2];
+  }
   for (uint32_t k = p0 + tid; k < p1; k += kFdaThreads) {
-    uint32_t ux = spos[3 * (int64_t)k + 0], uy = spos[3 * (int64_t)k + 1], uz = spos[3 * (int64_t)k + 2];
+    uint32_t kn = k + kFdaThreads, nx = 0, ny = 0, nz = 0;
+    if (kn < p1) {
+      nx = spos[3 * (int64_t)kn + 0];
+      ny = spos[3 * (int64_t)kn + 1];
+      nz = spos[3 * (int64_t)kn + 2];
+    }
     float3 f = fda_interp(gxy, gz, ux, uy, uz, nu, kPair ? 0u : half, x0, y0, z0);
     if (kPair) {
       // the mean of the two grids' forces
@@ -1224,6 +1244,9 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
     fpm[3 * (int64_t)k + 0] = f.x;
     fpm[3 * (int64_t)k + 1] = f.y;
     fpm[3 * (int64_t)k + 2] = f.z;
+    ux = nx;
+    uy = ny;
+    uz = nz;
   }
 }
 
