@@ -109,9 +109,11 @@ __global__ void __launch_bounds__(1024) k_radix_scan_digit(uint32_t *__restrict_
 // written out in that order, so each digit's run goes to consecutive global
 // addresses. Items of equal digit keep their input order (chunks in order,
 // lanes in order, warps in order), so the pass is a stable sort.
+// Three blocks per SM: the registers holding each lane's 16 keys and values
+// are budgeted so that the shared memory (57 KB per block) sets the occupancy.
 constexpr int kScatterWarps = kSortThreads / 32;
 constexpr int kWarpItems = kSortTile / kScatterWarps;
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
+__global__ void __launch_bounds__(kSortThreads, 3) k_radix_scatter(
     const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin, uint64_t *__restrict__ kout,
     uint32_t *__restrict__ vout, int64_t np, int shift, const uint32_t *__restrict__ hist,
     const uint32_t *__restrict__ dtotal, int64_t ntiles) {
@@ -128,12 +130,23 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
   __syncthreads();
   const int64_t tbase = blockIdx.x * (int64_t)kSortTile;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
+  // this lane's items of the warp's segment, all loaded before any is ranked
+  constexpr int kChunks = kWarpItems / 32;
+  uint64_t kr[kChunks];
+  uint32_t vr[kChunks];
+#pragma unroll
+  for (int c = 0; c < kChunks; c++) {
+    int64_t i = tbase + warp * kWarpItems + c * 32 + lane;
+    kr[c] = i < np ? kin[i] : 0ull;
+    vr[c] = i < np ? vin[i] : 0u;
+  }
   // ---- ranks inside each warp's segment
-  for (int c = 0; c < kWarpItems / 32; c++) {
+#pragma unroll
+  for (int c = 0; c < kChunks; c++) {
     int j = warp * kWarpItems + c * 32 + lane;
     int64_t i = tbase + j;
     bool valid = i < np;
-    uint32_t d = valid ? (uint32_t)(kin[i] >> shift) & 0xffu : 0x100u;
+    uint32_t d = valid ? (uint32_t)(kr[c] >> shift) & 0xffu : 0x100u;
     uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t prev = valid ? wc[warp][d] : 0u;
     __syncwarp();
@@ -179,15 +192,16 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
   }
   __syncthreads();
   // ---- place every item at its slot of the tile sorted by digit
-  for (int c = 0; c < kWarpItems / 32; c++) {
+#pragma unroll
+  for (int c = 0; c < kChunks; c++) {
     int j = warp * kWarpItems + c * 32 + lane;
     int64_t i = tbase + j;
     if (i < np) {
-      uint64_t k = kin[i];
+      uint64_t k = kr[c];
       uint32_t d = (uint32_t)(k >> shift) & 0xffu;
       uint32_t slot = lstart[d] + wc[warp][d] + rk[j];
       sk[slot] = k;
-      sv[slot] = vin[i];
+      sv[slot] = vr[c];
     }
   }
   __syncthreads();
