@@ -826,16 +826,34 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
   }
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, L, P, 1.f, a.radix, a.nf);
-  for (int p = 0; p < P; p++) {
-    int64_t row = row0 + p;
-    if (row >= nrows) break;
-    int y = (int)(row % n), z = (int)(row / n);
+  // threads run over (pencil, x) pairs of the block's rows, x in
+  // [-kGhost, n + kGhost) (n >= 16 > kGhost, so one wrap maps x into [0, n))
+  const int W = n + 2 * kGhost;
+  const float inv_w = 1.f / (float)W;
+  const int nrow = (int)min((int64_t)P, nrows - row0);
+  const int y0 = (int)(row0 % n), z0 = (int)(row0 / n);
+  for (int e = tid; e < nrow * W; e += nth) {
+    // p = e / W from the float reciprocal, corrected by one step
+    int p = (int)((float)e * inv_w);
+    int r = e - p * W;
+    if (r < 0) {
+      p--;
+      r += W;
+    } else if (r >= W) {
+      p++;
+      r -= W;
+    }
+    int y = y0 + p, z = z0;
+    while (y >= n) {
+      y -= n;
+      z++;
+    }
     // rows to write: (y, z) and its ghost copies
     int ys[2] = {y, y < kGhost ? y + n : (y >= n - kGhost ? y - n : 0x7fffffff)};
     int zs[2] = {z, z < kGhost ? z + n : (z >= n - kGhost ? z - n : 0x7fffffff)};
-    for (int e = tid; e < n + 2 * kGhost; e += nth) {
-      int x = e - kGhost;
-      int xs = (x % n + n) % n;
+    {
+      int x = r - kGhost;
+      int xs = x < 0 ? x + n : (x >= n ? x - n : x);
       float v;
       if (packed) {
         float2 c = res[p * L + (xs >> 1)];
