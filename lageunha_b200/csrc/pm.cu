@@ -304,6 +304,27 @@ static Factors factorize(int L, int rmax) {
   return f;
 }
 
+// Quotient by a divisor known only at run time, for 0 <= e < 2^24: a shift
+// where the divisor is a power of two (the usual mesh and batch sizes), else
+// the float reciprocal corrected by one step. The branch is uniform.
+struct Div {
+  int d, s;     // s >= 0: d == 1 << s
+  float inv;
+  TPM_D int q(int e) const {
+    if (s >= 0) return e >> s;
+    int p = (int)((float)e * inv);
+    int r = e - p * d;
+    return r < 0 ? p - 1 : (r >= d ? p + 1 : p);
+  }
+};
+TPM_D Div make_div(int d) {
+  Div r;
+  r.d = d;
+  r.s = (d & (d - 1)) == 0 ? __ffs(d) - 1 : -1;
+  r.inv = r.s >= 0 ? 0.f : 1.f / (float)d;
+  return r;
+}
+
 TPM_D float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 TPM_D float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 TPM_D float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -422,7 +443,8 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
     int p = job / jobs_per, j = job - p * jobs_per;
     const float2 *src = in + p * ld;
     float2 *dst = out + p * ld;
-    int k = j % Ns;
+    int jn = j / Ns;
+    int k = j - jn * Ns;
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
@@ -435,7 +457,7 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
       v[r] = x;
     }
     dft_small<R>(v, dir);
-    int d0 = (j / Ns) * Ns * R + k;
+    int d0 = jn * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; r++) dst[d0 + r * Ns] = v[r];
   }
@@ -545,12 +567,13 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
   for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
   int64_t row0 = (int64_t)blockIdx.x * P;
   bool packed = (L * 2 == n);
+  const Div dL = make_div(L), dH = make_div(hx);
   for (int e0 = tid; e0 < P * L; e0 += kLoadBatch * nth) {
     float2 v[kLoadBatch];
 #pragma unroll
     for (int u = 0; u < kLoadBatch; u++) {
       int e = e0 + u * nth;
-      int p = e / L, m = e - p * L;
+      int p = dL.q(e), m = e - p * L;
       int64_t row = row0 + p;
       v[u] = make_float2(0.f, 0.f);
       if (e < P * L && row < nrows) {
@@ -568,16 +591,16 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
   __syncthreads();
   float2 *res = fft_pencils(A, B, twl, L, L, P, -1.f, a.radix, a.nf);
   for (int e = tid; e < P * hx; e += nth) {
-    int p = e / hx, k = e - p * hx;
+    int p = dH.q(e), k = e - p * hx;
     int64_t row = row0 + p;
     if (row >= nrows) continue;
     float2 X;
     if (packed) {
       const float2 *Z = res + p * L;
-      float2 zk = Z[k % L], zc = cconj(Z[(L - k) % L]);
+      float2 zk = Z[k == L ? 0 : k], zc = cconj(Z[k == 0 ? 0 : L - k]);  // k <= L
       float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
       float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));  // times -i below
-      float2 w = tw_n[k % n];
+      float2 w = tw_n[k];  // k <= L < n
       float2 wo = cmul(w, make_float2(od.y, -od.x));
       X = cadd(ev, wo);
     } else {
@@ -681,13 +704,14 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
   int64_t stride = axis == 1 ? (int64_t)hx : (int64_t)n * hx;
   int64_t base = axis == 1 ? (int64_t)outer * n * hx : (int64_t)outer * hx;
   int tw_ = min(TX, hx - kx0);
+  const Div dP = make_div(P), dL = make_div(L);
   for (int e0 = tid; e0 < P * L; e0 += kLoadBatch * nth) {
     float2 v[kLoadBatch];
 #pragma unroll
     for (int u = 0; u < kLoadBatch; u++) {
       int e = e0 + u * nth;
-      int q = e % P, m = e / P;  // consecutive threads -> consecutive kx
-      int qs = q % TX;
+      int m = dP.q(e), q = e - m * P;  // consecutive threads -> consecutive kx
+      int qs = q < TX ? q : q - TX;
       const float2 *src = q < TX ? spec : spec2;
       v[u] = make_float2(0.f, 0.f);
       if (e < P * L && qs < tw_) v[u] = src[base + m * stride + kx0 + qs];
@@ -695,7 +719,8 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
 #pragma unroll
     for (int u = 0; u < kLoadBatch; u++) {
       int e = e0 + u * nth;
-      if (e < P * L) A[(e % P) * Lp + e / P] = v[u];
+      int m = dP.q(e);
+      if (e < P * L) A[(e - m * P) * Lp + m] = v[u];
     }
   }
   __syncthreads();
@@ -706,7 +731,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     __syncthreads();
     int wy = outer > n / 2 ? outer - n : outer;
     for (int e = tid; e < TX * L; e += nth) {
-      int q = e / L, m = e - q * L;
+      int q = dL.q(e), m = e - q * L;
       if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[q * Lp + m]);
     }
     __syncthreads();
@@ -716,7 +741,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
   if (with_green) {
     if (nspec == 1) {
       for (int e = tid; e < P * L; e += nth) {
-        int q = e / L, m = e - q * L;
+        int q = dL.q(e), m = e - q * L;
         float gk = green(ga, kx0 + q, outer, m);
         float2 v = res[q * Lp + m];
         res[q * Lp + m] = make_float2(v.x * gk, v.y * gk);
@@ -729,7 +754,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
 #pragma unroll
           for (int u = 0; u < kLoadBatch; u++) {
             int e = e0 + u * nth;
-            int q = e / L, m = e - q * L;
+            int q = dL.q(e), m = e - q * L;
             gks[u] = e < TX * L && kx0 + q < hx ? ga.gt[((int64_t)outer * hx + kx0 + q) * n + m] : 0.f;
           }
         }
@@ -737,7 +762,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
         for (int u = 0; u < kLoadBatch; u++) {
         int e = e0 + u * nth;
         if (e >= TX * L) break;
-        int q = e / L, m = e - q * L;
+        int q = dL.q(e), m = e - q * L;
         int kx = kx0 + q, wz = m > n / 2 ? m - n : m;
         float gk = ga.gt ? gks[u] : green(ga, kx, outer, m);
         if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
@@ -758,8 +783,8 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     res = fft_pencils(res, other, twl, L, Lp, P, 1.f, a.radix, a.nf);
   }
   for (int e = tid; e < P * L; e += nth) {
-    int q = e % P, m = e / P;
-    int qs = q % TX;
+    int m = dP.q(e), q = e - m * P;
+    int qs = q < TX ? q : q - TX;
     float2 *dst = q < TX ? spec : spec2;
     if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * Lp + m];
   }
@@ -781,12 +806,13 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
   int64_t row0 = (int64_t)blockIdx.x * P;
   bool packed = (L * 2 == n);
   constexpr int kB = kLoadBatch / 2;  // two loads per element
+  const Div dL = make_div(L);
   for (int e0 = tid; e0 < P * L; e0 += kB * nth) {
     float2 xa[kB], xb[kB];
 #pragma unroll
     for (int u = 0; u < kB; u++) {
       int e = e0 + u * nth;
-      int p = e / L, k = e - p * L;
+      int p = dL.q(e), k = e - p * L;
       int64_t row = row0 + p;
       xa[u] = xb[u] = make_float2(0.f, 0.f);
       if (e < P * L && row < nrows) {
@@ -803,7 +829,7 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
     for (int u = 0; u < kB; u++) {
       int e = e0 + u * nth;
       if (e >= P * L) break;
-      int k = e % L;
+      int k = e - dL.q(e) * L;
       float2 Zk;
       if (packed) {
         // Z_k = (X_k + conj X_{L-k}) + i conj(W^k) (X_k - conj X_{L-k})
