@@ -867,9 +867,12 @@ int tpm_read_forces(tpm_ctx *c, float *out, int mem) {
   if (!c || !out) return fail(TPM_E_ARG, "NULL argument");
   if (!c->parts_valid) return fail(TPM_E_STATE, "no forces computed");
   CK(cudaSetDevice(c->device));
-  k_finish<<<grid_for(c->np), 256, 0, c->st>>>(c->perm, c->np, c->fpm, c->ftree, c->parts_valid, c->fout);
+  // device memory takes the scatter to caller order directly; host memory
+  // gets it through the context's buffer
+  float *dst = mem == TPM_MEM_DEVICE ? out : c->fout;
+  k_finish<<<grid_for(c->np), 256, 0, c->st>>>(c->perm, c->np, c->fpm, c->ftree, c->parts_valid, dst);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(out, c->fout, sizeof(float) * 3 * c->np, kind_out(mem), c->st));
+  if (dst != out) CK(cudaMemcpyAsync(out, c->fout, sizeof(float) * 3 * c->np, kind_out(mem), c->st));
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }
