@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(1024) k_radix_scan_digit(uint32_t *__restrict_
 // addresses. Items of equal digit keep their input order (chunks in order,
 // lanes in order, warps in order), so the pass is a stable sort.
 // Three blocks per SM: the registers holding each lane's 16 keys and values
-// are budgeted so that the shared memory (57 KB per block) sets the occupancy.
+// are capped so that the shared memory (57 KB per block) sets the occupancy.
 constexpr int kScatterWarps = kSortThreads / 32;
 constexpr int kWarpItems = kSortTile / kScatterWarps;
 __global__ void __launch_bounds__(kSortThreads, 3) k_radix_scatter(

@@ -495,7 +495,7 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 
 // ------------------------------------------------------------------ walk
 constexpr int kWalkWarps = 16;
-constexpr int kWalkBlocksPerSm = 1;  // resident CTAs per SM the registers are budgeted for
+constexpr int kWalkBlocksPerSm = 1;  // resident CTAs per SM the registers are sized for
 constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr int kStackSmem = 640;    // per-warp stack entries in shared memory
 constexpr int kStackCap = 8192;    // entries beyond kStackSmem live in global memory
@@ -640,7 +640,7 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
   float2 a01x = make_float2(0.f, 0.f), a01y = a01x, a01z = a01x, a23x = a01x, a23y = a01x, a23z = a01x;
   // the rows of the next four sources are loaded before the arithmetic of
   // these four; past the last source that reads unused values still inside
-  // wl.stage (the z row ends 128 floats before it does)
+  // wl.stage (the z row ends 128 floats before the buffer does)
   int j = 0;
   if (m >= 4) {
     float4 x = *reinterpret_cast<const float4 *>(nsx);
