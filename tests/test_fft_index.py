@@ -1,0 +1,54 @@
+"""Index arithmetic of the FFT passes, checked on the CPU.
+
+The x and column passes of lageunha_b200/csrc/pm.cu take per-element
+quotients e / d by divisors known only at run time (pencil length L, row
+length n/2 + 1, batch width P, ghosted row width n + 16) through `Div`: a
+shift when d is a power of two, else p = trunc(float(e) * RN(1/d)) corrected
+by one step towards the exact quotient. This restates that arithmetic in
+IEEE float32 (numpy rounds float32 products and quotients to nearest, as the
+device does) and checks it against integer division at every quotient
+boundary e = k d - 1, k d, k d + 1 below the largest e any pass forms, for
+every divisor the passes use on meshes from 16 to 4096.
+"""
+import numpy as np
+
+# the largest e a pass forms: 64 pencils of a ghosted row of 4096 + 16
+# (the c2r write; the column passes form at most 32 * 4096)
+E_MAX = 64 * (4096 + 16)
+
+
+def _div_q(e, d):
+    """The device Div::q for 0 <= e < 2^24."""
+    if d & (d - 1) == 0:
+        return e >> (d.bit_length() - 1)
+    inv = np.float32(1.0) / np.float32(d)
+    p = (e.astype(np.float32) * inv).astype(np.int64)  # truncation, e >= 0
+    r = e - p * d
+    return np.where(r < 0, p - 1, np.where(r >= d, p + 1, p))
+
+
+def _divisors():
+    out = set()
+    for n in range(16, 4097):
+        half = n // 2
+        L = half if n % 2 == 0 else n
+        out.update({L, n // 2 + 1, n, n + 16})
+    for P in range(1, 65):
+        out.add(P)
+    return sorted(out)
+
+
+def test_quotient_matches_integer_division_at_every_boundary():
+    for d in _divisors():
+        k = np.arange(0, E_MAX // d + 2, dtype=np.int64)
+        e = np.concatenate([k * d - 1, k * d, k * d + 1])
+        e = e[(e >= 0) & (e < E_MAX)]
+        got = _div_q(e, d)
+        assert np.array_equal(got, e // d), d
+
+
+def test_quotient_on_random_elements():
+    rng = np.random.default_rng(3)
+    for d in (17, 45, 75, 81, 129, 135, 272, 2049, 4112):
+        e = rng.integers(0, E_MAX, size=200000, dtype=np.int64)
+        assert np.array_equal(_div_q(e, d), e // d), d
