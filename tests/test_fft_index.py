@@ -8,7 +8,9 @@ by one step towards the exact quotient. This restates that arithmetic in
 IEEE float32 (numpy rounds float32 products and quotients to nearest, as the
 device does) and checks it against integer division at every quotient
 boundary e = k d - 1, k d, k d + 1 below the largest e any pass forms, for
-every divisor the passes use on meshes from 16 to 4096.
+every divisor the passes use on meshes from 16 to 4096. The c2r pass's
+write phase, threads over (pencil, x) pairs, makes the same stores from the
+same transform outputs as one loop per pencil over x.
 """
 import numpy as np
 
@@ -52,3 +54,70 @@ def test_quotient_on_random_elements():
     for d in (17, 45, 75, 81, 129, 135, 272, 2049, 4112):
         e = rng.integers(0, E_MAX, size=200000, dtype=np.int64)
         assert np.array_equal(_div_q(e, d), e // d), d
+
+
+KGHOST = 8  # ghost layers of the padded potential
+
+
+def _c2r_writes_serial(n, P, row0, nrows, px, py):
+    """(offset, pencil, element) of every store of the x c2r pass's write
+    phase as one loop per pencil over x in [-KGHOST, n + KGHOST)."""
+    out = set()
+    for p in range(P):
+        row = row0 + p
+        if row >= nrows:
+            break
+        y, z = row % n, row // n
+        ys = [y, y + n if y < KGHOST else (y - n if y >= n - KGHOST else None)]
+        zs = [z, z + n if z < KGHOST else (z - n if z >= n - KGHOST else None)]
+        for e in range(n + 2 * KGHOST):
+            x = e - KGHOST
+            xs = (x % n + n) % n
+            for zz in zs:
+                for yy in ys:
+                    if zz is None or yy is None:
+                        continue
+                    out.add((x + KGHOST + px * ((yy + KGHOST) + py * (zz + KGHOST)), p, xs))
+    return out
+
+
+def _c2r_writes_flat(n, P, row0, nrows, px, py):
+    """The same stores as the kernel makes them: threads over (pencil, x)
+    pairs, p from the corrected float reciprocal, (y, z) by stepping from the
+    block's first row."""
+    W = n + 2 * KGHOST
+    inv_w = np.float32(1.0) / np.float32(W)
+    nrow = min(P, nrows - row0)
+    y0, z0 = row0 % n, row0 // n
+    out = set()
+    for e in range(nrow * W):
+        p = int(np.float32(e) * inv_w)
+        r = e - p * W
+        if r < 0:
+            p, r = p - 1, r + W
+        elif r >= W:
+            p, r = p + 1, r - W
+        y, z = y0 + p, z0
+        while y >= n:
+            y, z = y - n, z + 1
+        ys = [y, y + n if y < KGHOST else (y - n if y >= n - KGHOST else None)]
+        zs = [z, z + n if z < KGHOST else (z - n if z >= n - KGHOST else None)]
+        x = r - KGHOST
+        xs = x + n if x < 0 else (x - n if x >= n else x)
+        for zz in zs:
+            for yy in ys:
+                if zz is None or yy is None:
+                    continue
+                out.add((x + KGHOST + px * ((yy + KGHOST) + py * (zz + KGHOST)), p, xs))
+    return out
+
+
+def test_c2r_flat_write_covers_the_serial_loop():
+    for n, P in ((16, 8), (16, 64), (20, 32), (32, 16), (45, 64), (64, 64)):
+        px = ((n + 2 * KGHOST) + 3) // 4 * 4
+        py = n + 2 * KGHOST
+        nrows = n * n
+        for row0 in range(0, nrows, P):
+            a = _c2r_writes_serial(n, P, row0, nrows, px, py)
+            b = _c2r_writes_flat(n, P, row0, nrows, px, py)
+            assert a == b, (n, P, row0)
