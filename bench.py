@@ -610,8 +610,14 @@ def run_engine_arm(args):
                                    f"interaction evaluated: {counters['pp']} and {counters['pc']} per launch"}
     else:
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": None, "peak": hbm_peak, "unit": "GB/s"}
-    # HBM-bound stages: algorithmic bytes per particle (each stage's minimal reads and writes)
-    bytes_pp = {"sort": 28 + 5 * 32, "deposit": 16, "fft": 16 * n ** 3 / npart, "fda4": 28}
+    # HBM-bound stages: algorithmic bytes per particle (each stage's minimal reads and
+    # writes): positions read once and forces written once per stage that uses them, and
+    # each of the PM's grids (two interlaced ones for the Gaussian law) written by the
+    # deposit, read and written once per transform, read by fda4
+    grids = 1 if args.law == "reference" else 2
+    mesh_pp = 4 * n ** 3 / npart
+    bytes_pp = {"sort": 28 + 5 * 32, "deposit": 12 + grids * mesh_pp, "fft": grids * 4 * mesh_pp,
+                "fda4": 24 + grids * mesh_pp}
     hbm_stages = {}
     for k, b in bytes_pp.items():
         if per.get(k, 0) > 0:
