@@ -44,7 +44,10 @@ std::mutex g_setup_mutex;
 void *g_scratch_addr[kMaxDevices] = {nullptr};
 
 // The device address of this device's scratch, looked up once per device
-// with that device current (the calling thread's current device).
+// with that device current (the calling thread's current device). It is kept
+// for the life of the process: after a cudaDeviceReset the module is loaded
+// again in a new context and the kept address would be stale, so the entry
+// point is documented as not for use on a device after its reset.
 cudaError_t scratch_for_device(int dev, unsigned char **out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_addr[dev]) {

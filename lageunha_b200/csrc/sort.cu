@@ -224,11 +224,9 @@ void radix_sort_pairs(uint64_t **key, uint32_t **val, uint64_t *key_alt, uint32_
   if (np <= 1) return;
   uint64_t *kin = *key, *kout = key_alt;
   uint32_t *vin = *val, *vout = val_alt;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem);
-    attr_set = true;
-  }
+  // the cap is an attribute of the function on the current device: raised on
+  // every call, so contexts and threads on any device get it
+  cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScatterSmem);
   for (int shift = 0; shift < nbits; shift += 8) {
     k_radix_hist<<<(unsigned)ntiles, kSortThreads, 0, st>>>(kin, np, shift, scr.hist, ntiles);
     k_radix_scan_digit<<<256, 1024, 0, st>>>(scr.hist, ntiles, scr.dtotal);

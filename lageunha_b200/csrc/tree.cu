@@ -1000,15 +1000,12 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
 }
 
 static int walk_grid(size_t smem) {
-  // The dynamic shared-memory cap is raised once (the tables and the warp
-  // records have fixed sizes, the same for every law and context).
-  static int cap_set = 0;
-  if (!cap_set) {
-    size_t max_smem = sizeof(float4) * (kLogSmemF4 + kPcEntries + 1) + sizeof(WarpLists) * kWalkWarps;
-    cudaFuncSetAttribute(k_tree_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
-    cudaFuncSetAttribute(k_tree_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
-    cap_set = 1;
-  }
+  // The dynamic shared-memory cap is an attribute of the function on the
+  // current device: it is raised on every launch, so every device (and every
+  // host thread) gets it.
+  size_t max_smem = sizeof(float4) * (kLogSmemF4 + kPcEntries + 1) + sizeof(WarpLists) * kWalkWarps;
+  cudaFuncSetAttribute(k_tree_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+  cudaFuncSetAttribute(k_tree_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tree_walk<true>, kWalkThreads, smem);
   int dev = 0, sms = 148;

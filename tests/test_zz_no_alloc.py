@@ -63,6 +63,22 @@ def test_noalloc_order_matches_engine_twice():
         assert np.array_equal(p_na.astype(np.int64), order), name
 
 
+def test_noalloc_ragged_and_single_particle():
+    """Counts that are not a multiple of the sort's 4096-particle tile (the
+    partial last tile), a single particle (the sort returns at once and the
+    keys and indices reach the caller's buffers by a copy), and a mesh that
+    is not a power of two."""
+    rng = np.random.default_rng(17)
+    for np_, n in [(100003, 64), (1, 32), (54321, 48)]:
+        pu = rng.integers(0, 2 ** 32, size=(np_, 3), dtype=np.uint64).astype(np.uint32)
+        for _ in range(2):
+            k_na, p_na = _noalloc_order(n, pu)
+            k_ref = O.morton_keys(pu, n)
+            order = O.sort_order(k_ref)
+            assert np.array_equal(p_na.astype(np.int64), order), (np_, n)
+            assert np.array_equal(k_na, k_ref[order]), (np_, n)
+
+
 def test_noalloc_rejects_oversize_and_bad_arguments():
     import torch
 
