@@ -239,3 +239,25 @@ def test_full_size_properties_clustered256():
     assert abs(rho.astype(np.float64).sum() - ps.np) < 1e-4 * ps.np
     assert np.all(np.isfinite(f))
     assert cnt["nodes"] > 0 and cnt["pp"] > 0
+
+
+def test_contexts_on_every_visible_device():
+    """Kernels with a raised dynamic shared-memory cap (the radix scatter,
+    the tree walk) launch on every device of the process: the cap is a
+    per-device attribute. Skips when only one device is visible."""
+    import torch
+
+    ndev = torch.cuda.device_count()
+    if ndev < 2:
+        pytest.skip("one visible device")
+    n = 32
+    ps, pu, pos = _case("clustered256", n)
+    ref = None
+    for d in range(ndev):
+        with _engine(n, device=d) as eng:
+            eng.load_fixed(pu)
+            eng.compute(E.PART_ALL)
+            f = eng.forces()
+        if ref is None:
+            ref = f
+        assert np.max(O.rel_err(f, ref)) <= 1e-4, d
