@@ -81,6 +81,9 @@ void tpm_default_params(tpm_params *p, int32_t n_mesh);
 const char *tpm_last_error(void);
 const char *tpm_version(void);
 
+/* Number of CUDA devices visible to the process (0 when there is none). */
+int tpm_device_count(void);
+
 /* Create a context on CUDA device `device` with capacity for up to np_max
  * particles (device memory is reserved lazily and grown on demand). */
 int tpm_create(const tpm_params *params, int device, tpm_ctx **out);
@@ -181,6 +184,39 @@ int tpm_hubble_drag(tpm_ctx *ctx, float fact1);
  * angle follows TreeAndPreFoFmain's step schedule (Cosmos/globalT.c:41-44).
  * The caller advances anow by astep afterwards. */
 int tpm_step(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t stepcount);
+
+/* PMSTATUS of the reference (eunha.h:72-77). */
+#define TPM_PUSH 0
+#define TPM_PULL 1
+#define TPM_KICK 2
+
+/* The factors one status applies (replaces the selections of
+ * PM_PULL_AND_PUSH, Cosmos/globalT.c:119-127, fda4, Cosmos/fda4.c:48-62, and
+ * TREE_HALF, Cosmos/indT.h:98-118):
+ *   drag     KICK fact1, PULL fact1_pull, PUSH fact1_push;
+ *   pm_kick  KICK fact2, PULL fact2_pull, PUSH fact2_push / GetFact1(anow,
+ *            anow + astep/2), which is fact2_push / fact1_push;
+ *   tree_kick  fact2 in every status: TREE_HALF stores the full-step fact2
+ *            for PULL and for the PUSH half's KICK call alike.
+ * Any output pointer may be NULL. Host only. */
+int tpm_status_factors(const tpm_evolfact *e, int32_t status, float *drag, float *pm_kick, float *tree_kick);
+
+/* One status of a global step on the particles the context holds (the body
+ * of PM_PULL_AND_PUSH plus TreeAndPreFoFmain's tree kick,
+ * Cosmos/globalT.c:113-134,85-87): v *= drag, then v += pm_kick F_pm +
+ * tree_kick F_tree with the factors of tpm_status_factors. The forces are
+ * evaluated unless the context already holds them for the current positions
+ * (the PUSH half of a synchronisation step reuses the PULL half's forces: the
+ * positions have not moved). No drift. */
+int tpm_status_kick(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t status);
+
+/* One global step of GOTPM_Cosmos_GlobalT (Cosmos/globalT.c:221-305) with
+ * the reference's status sequencing: sync == 0, KICK; sync != 0 (a
+ * synchronisation or PreFoF step, flagsyncpdata/flagPreFoF), PULL then
+ * PUSH; then the drift with pfact. The opening-angle schedule is tpm_step's.
+ * The caller advances anow by astep afterwards. */
+int tpm_global_step(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t stepcount,
+                    int32_t sync);
 
 /* ---- captured evaluations and ensembles ---- */
 
@@ -456,8 +492,10 @@ int tpm_ic_2lpt(const tpm_ic_params *p, void *records, int mem);
  * TPM_NOALLOC_MAX_PARTICLES is rejected with TPM_E_ARG. The first call on a
  * device looks up the device address of its scratch (cudaGetSymbolAddress,
  * with that device current), so make that first call before any stream
- * capture. All calls share the one scratch array: calls whose work overlaps
- * on the GPU race and must be serialised by the caller. */
+ * capture. The address is kept for the life of the process, so a caller that
+ * resets a device (cudaDeviceReset) must not call this entry point on that
+ * device afterwards. All calls share the one scratch array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller. */
 int tpm_morton_order_noalloc(const uint32_t *pos, int64_t np, int32_t n_mesh, uint64_t *keys,
                              uint32_t *perm, void *stream);
 

@@ -532,6 +532,15 @@ int tpm::launch_drift(tpm_ctx *c, cudaStream_t st, double pfact, const double *f
 
 extern "C" {
 
+int tpm_device_count(void) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return ndev;
+}
+
 int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
   if (!out) return fail(TPM_E_ARG, "out is NULL");
   *out = nullptr;

@@ -229,6 +229,75 @@ int tpm_step(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, 
   return rc;
 }
 
+int tpm_status_factors(const tpm_evolfact *e, int32_t status, float *drag, float *pm_kick, float *tree_kick) {
+  if (!e || (status != TPM_KICK && status != TPM_PULL && status != TPM_PUSH)) {
+    tpm::set_last_error("bad arguments to tpm_status_factors");
+    return TPM_E_ARG;
+  }
+  float f1, f2;
+  if (status == TPM_PUSH) {
+    // fda4 divides fact2_push by GetFact1(anow, anow + astep/2), the same
+    // float call that made fact1_push
+    f1 = e->fact1_push;
+    f2 = e->fact2_push / e->fact1_push;
+  } else if (status == TPM_PULL) {
+    f1 = e->fact1_pull;
+    f2 = e->fact2_pull;
+  } else {
+    f1 = e->fact1;
+    f2 = e->fact2;
+  }
+  if (drag) *drag = f1;
+  if (pm_kick) *pm_kick = f2;
+  if (tree_kick) *tree_kick = e->fact2;
+  return 0;
+}
+
+int tpm_status_kick(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t status) {
+  if (!ctx || !cosmo) return tpm::fail(TPM_E_ARG, "tpm_status_kick: NULL argument");
+  if (ctx->np <= 0) return tpm::fail(TPM_E_STATE, "no particles loaded");
+  tpm_evolfact e;
+  int rc = tpm_evol_factors(cosmo, ctx->prm.n_mesh, anow, astep, &e);
+  if (rc) return rc;
+  float drag, f2pm, f2tree;
+  rc = tpm_status_factors(&e, status, &drag, &f2pm, &f2tree);
+  if (rc) return rc;
+  // the drag does not move particles: forces of the current positions stay
+  // valid across it
+  rc = tpm_hubble_drag(ctx, drag);
+  if (!rc && (ctx->parts_valid & TPM_PART_ALL) != TPM_PART_ALL) rc = tpm_compute_forces(ctx, TPM_PART_ALL);
+  if (!rc) rc = tpm_kick(ctx, f2pm, f2tree);
+  return rc;
+}
+
+int tpm_global_step(tpm_ctx *ctx, const tpm_cosmology *cosmo, float anow, float astep, int32_t stepcount,
+                    int32_t sync) {
+  if (!ctx || !cosmo) return tpm::fail(TPM_E_ARG, "tpm_global_step: NULL argument");
+  if (!sync) return tpm_step(ctx, cosmo, anow, astep, stepcount);
+  tpm_params p;
+  int rc = tpm_get_params(ctx, &p);
+  if (rc) return rc;
+  if (p.law == TPM_LAW_REFERENCE) {
+    float th = tpm::theta_schedule(stepcount);
+    if (th != p.theta) {
+      p.theta = th;
+      rc = tpm_set_params(ctx, &p);
+      if (rc) return rc;
+    }
+  }
+  // a synchronisation step: PULL (the velocities reach anow), then PUSH on
+  // the same positions and forces, then the drift (Cosmos/globalT.c:244-291)
+  ctx->parts_valid = 0;
+  rc = tpm_status_kick(ctx, cosmo, anow, astep, TPM_PULL);
+  if (!rc) rc = tpm_status_kick(ctx, cosmo, anow, astep, TPM_PUSH);
+  if (!rc) {
+    tpm_evolfact e;
+    rc = tpm_evol_factors(cosmo, p.n_mesh, anow, astep, &e);
+    if (!rc) rc = tpm_drift(ctx, e.pfact);
+  }
+  return rc;
+}
+
 }  // extern "C"
 
 float tpm::theta_schedule(int stepcount) {

@@ -116,6 +116,7 @@ _SIGS = {
     "tpm_default_params": (None, [ctypes.POINTER(TpmParams), ctypes.c_int32]),
     "tpm_last_error": (ctypes.c_char_p, []),
     "tpm_version": (ctypes.c_char_p, []),
+    "tpm_device_count": (ctypes.c_int, []),
     "tpm_create": (ctypes.c_int, [ctypes.POINTER(TpmParams), ctypes.c_int, ctypes.POINTER(_P)]),
     "tpm_destroy": (ctypes.c_int, [_P]),
     "tpm_set_params": (ctypes.c_int, [_P, ctypes.POINTER(TpmParams)]),
@@ -168,6 +169,12 @@ _SIGS = {
                                         ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
     "tpm_hubble_drag": (ctypes.c_int, [_P, ctypes.c_float]),
     "tpm_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float, ctypes.c_int32]),
+    "tpm_status_factors": (ctypes.c_int, [ctypes.POINTER(TpmEvolFact), ctypes.c_int32, ctypes.POINTER(ctypes.c_float),
+                                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "tpm_status_kick": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_int32]),
+    "tpm_global_step": (ctypes.c_int, [_P, ctypes.POINTER(TpmCosmology), ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_int32, ctypes.c_int32]),
     "tpm_stream_submit": (ctypes.c_int, [_P, _I64, _P, _P, ctypes.c_uint, ctypes.POINTER(ctypes.c_int64)]),
     "tpm_stream_wait": (ctypes.c_int, [_P, _I64]),
     "tpm_ic_noise": (ctypes.c_int, [ctypes.POINTER(TpmIcParams), _P, ctypes.c_int]),
@@ -414,6 +421,16 @@ class Engine:
         """One GOTPM global step in KICK status (Cosmos/globalT.c:221-305)."""
         _check(self._lib.tpm_step(self._ctx, ctypes.byref(cosmo), anow, astep, stepcount))
 
+    def status_kick(self, cosmo: TpmCosmology, anow: float, astep: float, status: int):
+        """Drag and kicks of one PMSTATUS (PUSH 0, PULL 1, KICK 2): the body of
+        PM_PULL_AND_PUSH plus the tree kick (Cosmos/globalT.c:113-134)."""
+        _check(self._lib.tpm_status_kick(self._ctx, ctypes.byref(cosmo), anow, astep, status))
+
+    def global_step(self, cosmo: TpmCosmology, anow: float, astep: float, stepcount: int, sync: bool = False):
+        """One global step with the reference's sequencing: KICK, or PULL then
+        PUSH at a synchronisation step, then the drift (globalT.c:221-305)."""
+        _check(self._lib.tpm_global_step(self._ctx, ctypes.byref(cosmo), anow, astep, stepcount, int(bool(sync))))
+
     # ---------------------------------------------------------------- diagnostics
     def ewald(self, targets) -> np.ndarray:
         t = np.ascontiguousarray(targets, dtype=np.int64)
@@ -575,6 +592,19 @@ def evol_factors(cosmo: TpmCosmology, nx: int, anow: float, astep: float) -> dic
     out = TpmEvolFact()
     _check(load_library().tpm_evol_factors(ctypes.byref(cosmo), nx, anow, astep, ctypes.byref(out)))
     return {k: getattr(out, k) for k, _ in TpmEvolFact._fields_}
+
+
+PUSH, PULL, KICK = 0, 1, 2  # PMSTATUS (eunha.h:72-77)
+
+
+def status_factors(cosmo: TpmCosmology, nx: int, anow: float, astep: float, status: int) -> tuple:
+    """(drag, pm_kick, tree_kick) of one status (tpm_status_factors)."""
+    lib = load_library()
+    e = TpmEvolFact()
+    _check(lib.tpm_evol_factors(ctypes.byref(cosmo), nx, anow, astep, ctypes.byref(e)))
+    d, p, t = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    _check(lib.tpm_status_factors(ctypes.byref(e), status, ctypes.byref(d), ctypes.byref(p), ctypes.byref(t)))
+    return d.value, p.value, t.value
 
 
 def read_snapshot(path: str):

@@ -70,6 +70,7 @@ def ref(variant: int = VARIANT_B):
         L.ref_potential.argtypes = [_int, _i64, _u64p, _f32p, _flt, _f32p]
         L.ref_spline_table.argtypes = [_int, _flt, _f64p, _f64p]
         L.ref_evol_factors.argtypes = [_int, _flt, _flt, _flt, _flt, _flt, _flt, _flt, _f32p]
+        L.ref_status_kick.argtypes = [_int, _i64, _u64p, _f32p, _f32p] + [_flt] * 11 + [_int]
         L.ref_write_snapshot.argtypes = [ctypes.c_char_p, _int, ctypes.c_int64, ctypes.c_void_p] + [_flt] * 5 + \
             [ctypes.c_double] * 2 + [_flt] * 4 + [_int]
         L.ref_read_head.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
@@ -77,6 +78,44 @@ def ref(variant: int = VARIANT_B):
                                          ctypes.c_void_p]
         _ref[variant] = L
     return _ref[variant]
+
+
+_dropin = None
+
+
+def dropin_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libgotpm_dropin.so"))
+
+
+def dropin():
+    """The engine's legacy-name entry points (lageunha_b200/gotpm/tpm_gotpm.c)
+    built against the reference's eunha.h with the harness dropin_shim.c."""
+    global _dropin
+    if _dropin is None:
+        path = os.path.join(HERE, "_ref", "libgotpm_dropin.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is not built (needs the reference tree; `make -C oracle ref`)")
+        L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        L.dropin_pmmain.argtypes = [_int, _i64, _u64p, _f32p, _f32p, _f32p, _int, _flt, _flt]
+        L.dropin_treemain.argtypes = [_int, _i64, _u64p, _f32p, _f32p, _flt, _flt, _int, _flt, _flt]
+        _dropin = L
+    return _dropin
+
+
+def dropin_pmmain(n, indx, off, vel, evolfact9, status, efold=0.9, eps=0.05):
+    """The drop-in pmmain(SimParameters*, EvolFact): returns (status, velocities)."""
+    v = np.array(vel, dtype=np.float32, order="C", copy=True)
+    ef = np.ascontiguousarray(evolfact9, dtype=np.float32)
+    rc = dropin().dropin_pmmain(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), v, ef, status, efold, eps)
+    return rc, v
+
+
+def dropin_treemain(n, indx, off, vel, fact1, fact2, stepcount, rsphere=4.0, eps=0.05):
+    """The drop-in TreeMain(SimParameters*, DeterminedEvolFact*)."""
+    v = np.array(vel, dtype=np.float32, order="C", copy=True)
+    rc = dropin().dropin_treemain(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), v, fact1, fact2,
+                                  stepcount, rsphere, eps)
+    return rc, v
 
 
 def _c(a, dt):
@@ -159,6 +198,16 @@ def ref_tree_force(n, indx, off, theta=0.3, rsphere=4.0, eps=0.05, variant=VARIA
     ref(variant).ref_tree_force(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), theta,
                                 rsphere, eps, out)
     return out
+
+
+def ref_status_kick(n, indx, off, vel, status, anow, astep, cosmo=(0.26, 0.74, -1.0, 0.0, 48.0), efold=0.9,
+                    theta=0.3, rsphere=4.0, eps=0.05, variant=VARIANT_B):
+    """One PMSTATUS half of the reference's global step (drag, pmmain, tree
+    kick with the full-step fact2): returns the new velocities."""
+    v = np.array(vel, dtype=np.float32, order="C", copy=True)
+    ref(variant).ref_status_kick(n, indx.shape[0], _c(indx, np.uint64), _c(off, np.float32), v, efold, theta,
+                                 rsphere, eps, *[float(c) for c in cosmo], anow, astep, status)
+    return v
 
 
 def ref_tsc_density(n, indx, off):

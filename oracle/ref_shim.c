@@ -418,6 +418,70 @@ int ref_spline_table(int n, float eps, double *diff_out, double *slope_out) {
 
 int ref_nspline(void) { return NSPLINE; }
 
+/* One PMSTATUS half of the reference's global step on one rank's particles,
+ * velocities in and out: PM_PULL_AND_PUSH (Cosmos/globalT.c:113-134: drag
+ * v *= fact1 of the status, then the reference's own pmmain, whose fda4
+ * picks fact2 by PMSTATUS and divides PUSH's by GetFact1, Cosmos/fda4.c:
+ * 48-62), then TreeAndPreFoFmain's tree kick (TREE_HALF, Cosmos/indT.h:
+ * 98-118: the full-step fact2 of GetEvolFactor) through the reference's own
+ * treecorrection. The drag and the factor selection are restated here
+ * because globalT.c does not build on one rank. */
+int ref_status_kick(int n, int64_t np, const uint64_t *indx, const float *off, float *vel, float efold,
+                    float theta, float rsphere, float eps, float omep, float omeplam, float wlam0, float wlam1,
+                    float amax, float anow, float astep, int status) {
+  RefBox *b = refbox_new(n, efold, eps, theta, rsphere);
+  SimParameters *s = &b->sim;
+  OMEP(s) = omep;
+  OMEPLAM(s) = omeplam;
+  WLAM0(s) = wlam0;
+  WLAM1(s) = wlam1;
+  AMAX(s) = amax;
+  ANOW(s) = anow;
+  ASTEP(s) = astep;
+  PMSTATUS(s) = status;
+  STEPCOUNT(s) = 2;
+  EvolFact e = GetEvolFactor(s);
+  float vfact1 = status == PUSH ? e.fact1_push : (status == PULL ? e.fact1_pull : e.fact1);
+  dmparticletype *p = (dmparticletype *)calloc((size_t)np, sizeof(dmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    set_index(&p[i].u4if, indx[i]);
+    p[i].x = off[3 * i];
+    p[i].y = off[3 * i + 1];
+    p[i].z = off[3 * i + 2];
+    p[i].vx = vel[3 * i] * vfact1;
+    p[i].vy = vel[3 * i + 1] * vfact1;
+    p[i].vz = vel[3 * i + 2] * vfact1;
+  }
+  DM_NP(s) = np;
+  DM_BP(s) = p;
+  pmmain(s, e);
+  treedmparticletype *t = (treedmparticletype *)calloc((size_t)np, sizeof(treedmparticletype));
+  for (int64_t i = 0; i < np; i++) {
+    t[i].u4if = p[i].u4if;
+    t[i].x = p[i].x;
+    t[i].y = p[i].y;
+    t[i].z = p[i].z;
+    t[i].vx = p[i].vx;
+    t[i].vy = p[i].vy;
+    t[i].vz = p[i].vz;
+  }
+  DM_TBP(s) = t;
+  DeterminedEvolFact ef[1];
+  ef[0].fact1 = e.fact1;
+  ef[0].fact2 = e.fact2;
+  initflag = 0;
+  treecorrection(s, ef);
+  for (int64_t i = 0; i < np; i++) {
+    vel[3 * i] = t[i].vx;
+    vel[3 * i + 1] = t[i].vy;
+    vel[3 * i + 2] = t[i].vz;
+  }
+  free(t);
+  free(p);
+  free(b);
+  return 0;
+}
+
 /* GetEvolFactor (Cosmos/CosmosEvolFactor.c:230-255) for one cosmology:
  * out = {afact, bfact, pfact, fact1, fact2, fact1_push, fact2_push,
  * fact1_pull, fact2_pull} (the EvolFact field order, CosmosEvolFactor.h:1-6). */

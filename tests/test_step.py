@@ -137,3 +137,79 @@ def test_hubble_drag_scales_velocities_exactly():
         eng.hubble_drag(0.987654)
         v = eng.velocities()
     assert np.array_equal(v, vel * np.float32(0.987654))
+
+
+# ---------------------------------------------------------------- PMSTATUS
+def test_status_factors_follow_the_reference_selection():
+    """tpm_status_factors picks what PM_PULL_AND_PUSH (Cosmos/globalT.c:
+    119-127), fda4 (Cosmos/fda4.c:48-62) and TREE_HALF (Cosmos/indT.h:
+    98-118) pick: the drag and PM factors by status, PUSH's PM factor divided
+    by GetFact1(anow, anow + astep/2) = fact1_push, and the full-step fact2
+    for the tree in every status. Host only."""
+    c = E.cosmology()
+    nx, anow, astep = 64, 3.0, 0.25
+    e = E.evol_factors(c, nx, anow, astep)
+    f32 = np.float32
+    assert E.status_factors(c, nx, anow, astep, E.KICK) == (e["fact1"], e["fact2"], e["fact2"])
+    assert E.status_factors(c, nx, anow, astep, E.PULL) == (e["fact1_pull"], e["fact2_pull"], e["fact2"])
+    d, p, t = E.status_factors(c, nx, anow, astep, E.PUSH)
+    assert d == e["fact1_push"] and t == e["fact2"]
+    assert f32(p) == f32(f32(e["fact2_push"]) / f32(e["fact1_push"]))
+
+
+def _status_case():
+    n = 32
+    ps = ic.workload("clustered256", scale=n)
+    vel = (0.05 * np.random.default_rng(5).standard_normal((ps.np, 3))).astype(np.float32)
+    return n, ps, vel
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not O.ref_available(O.VARIANT_B), reason="oracle/_ref not built (reference tree absent)")
+@pytest.mark.parametrize("status", [E.KICK, E.PULL, E.PUSH])
+def test_status_kick_vs_reference_build(status):
+    """One status half of the global step against the reference's own
+    pmmain and treecorrection run with PMSTATUS set (variant B): the velocity
+    change beyond the drag, per particle, within the force bar (rms 1e-3,
+    99th percentile 1e-2)."""
+    n, ps, vel = _status_case()
+    c = E.cosmology()
+    anow, astep = 2.0, 0.2
+    with E.Engine(n, epsilon=0.05) as eng:
+        eng.load_fixed(ps.positions_u32(), vel)
+        eng.status_kick(c, anow, astep, status)
+        v_eng = eng.velocities()
+    v_ref = O.ref_status_kick(n, ps.indx, ps.offset, vel, status, anow, astep)
+    drag = np.float32(E.status_factors(c, n, anow, astep, status)[0])
+    base = vel * drag
+    e = O.rel_err(v_eng.astype(np.float64) - base, v_ref.astype(np.float64) - base)
+    assert float(np.sqrt(np.mean(e * e))) <= 1e-3
+    assert float(np.percentile(e, 99)) <= 1e-2
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not O.ref_available(O.VARIANT_B), reason="oracle/_ref not built (reference tree absent)")
+def test_sync_step_is_pull_then_push_then_drift():
+    """A synchronisation step (tpm_global_step with sync) is the reference's
+    PULL half, then its PUSH half on the same positions, then the drift
+    (Cosmos/globalT.c:244-291)."""
+    n, ps, vel = _status_case()
+    c = E.cosmology()
+    anow, astep = 2.0, 0.2
+    pu = ps.positions_u32()
+    with E.Engine(n, epsilon=0.05) as eng:
+        eng.load_fixed(pu, vel)
+        eng.global_step(c, anow, astep, 2, sync=True)
+        v_eng = eng.velocities()
+        p_eng = eng.positions()
+    v1 = O.ref_status_kick(n, ps.indx, ps.offset, vel, E.PULL, anow, astep)
+    v2 = O.ref_status_kick(n, ps.indx, ps.offset, v1, E.PUSH, anow, astep)
+    d1 = np.float32(E.status_factors(c, n, anow, astep, E.PULL)[0])
+    d2 = np.float32(E.status_factors(c, n, anow, astep, E.PUSH)[0])
+    base = vel * d1 * d2
+    e = O.rel_err(v_eng.astype(np.float64) - base, v2.astype(np.float64) - base)
+    assert float(np.sqrt(np.mean(e * e))) <= 1e-3
+    assert float(np.percentile(e, 99)) <= 1e-2
+    pfact = E.evol_factors(c, n, anow, astep)["pfact"]
+    dq = np.rint(np.fmod(v_eng.astype(np.float64) * pfact * (2.0 ** 32 / n), 2.0 ** 32)).astype(np.int64)
+    assert np.array_equal(p_eng, ((pu.astype(np.int64) + dq) % (2 ** 32)).astype(np.uint32))
