@@ -3,21 +3,24 @@
 
 One step = one full TreePM force evaluation (Morton sort, TSC deposit,
 Poisson FFT, gradient + interpolation, tree build, tree walk, forces
-scattered back to the caller's order) of the clustered 256^3 workload:
-256^3 particles on a 256^3 mesh, L = 200 Mpc/h, Zel'dovich field with
-P(k) ~ k^-2 exp(-(0.5k)^2) and 1.5-spacing rms displacement plus 200 Plummer
-spheres (a = 0.64 cells, 2000-20000 particles each), softening 0.05 cells,
-theta 0.3.
+scattered back to the caller's order) of the plain engine at scale: 512^3
+particles on a 512^3 mesh, L = 500 Mpc/h, seeded Zel'dovich field with
+P(k) ~ k^-2.5 and an rms displacement of 2 spacings (strongly clustered),
+velocities 0.5 psi, softening 0.05 cells.
 
 The metric is quoted at rms force error <= 1e-3 against the FP64 Ewald sum.
 The reference's own split law (PMFITPARA residual, efold 0.9, rsphere 4)
-stays near 3.5e-3 on this workload, so the headline uses the engine's
+stays near 3.5e-3 on these workloads, so the headline uses the engine's
 Gaussian split (rs = 0.7 cells, short-range cut at 3.5 cells, interlaced
 TSC grids with their optimal influence function, 8-point gradient, theta
-0.5: rms 8e-4 here, 7e-4 on the 512^3 workload); the same line also carries the
-reference law's throughput and error ("reference_law"), one KDK global step
-("kdk_step_ms"), the 64-box uneven ensemble evaluated box by box and batched
-("ensemble"), and the served request loop ("served").
+0.4: rms 4.8e-4 at 512^3 and below 8e-4 on every workload the tests run);
+the same line also carries the reference law's throughput and error
+("reference_law"), ten KDK global steps ("kdk"), the clustered 256^3
+workload ("clustered256"), cuFFT timed on the same transforms
+("fft_check"), the whole-step roofline ("step_roofline"), the 64-box uneven
+ensemble evaluated box by box and batched ("ensemble"), the served request
+loop ("served") and the engine's error against the reference build on the
+CPU sample ("parity_vs_reference").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -46,11 +49,20 @@ sys.path.insert(0, ROOT)
 METRIC = "Mparticles/s per TreePM force eval (plain vs batched) at rms err≤1e-3; p50/p99 latency"
 UNIT = "Mparticles/s"
 EPS = 0.05
-HEADLINE_LAW = {"law": "gaussian", "rs_split": 0.7, "rsphere": 3.5, "theta": 0.5, "efold": 0.9}
+HEADLINE_LAW = {"law": "gaussian", "rs_split": 0.7, "rsphere": 3.5, "theta": 0.4, "efold": 0.9}
 # weakly clustered boxes carry small net forces: the ensemble and the served
 # requests open nodes more often to stay under the same error bar
 BOX_LAW = {"law": "gaussian", "rs_split": 0.8, "rsphere": 4.0, "theta": 0.3, "efold": 0.9}
 REFERENCE_LAW = {"law": "reference", "rs_split": 1.25, "rsphere": 4.0, "theta": 0.3, "efold": 0.9}
+WORKLOADS = {
+    "scale512": "scale512: 512^3 particles on a 512^3 mesh, L=500 Mpc/h, Zel'dovich field P(k)~k^-2.5, "
+                "rms displacement 2 spacings, v=0.5 psi",
+    "clustered256": "clustered256: 256^3 particles on a 256^3 mesh, L=200 Mpc/h, Zel'dovich field "
+                    "P(k)~k^-2 exp(-(0.5k)^2), rms 1.5 spacings, plus 200 Plummer spheres (a=0.64 cells, "
+                    "2000-20000 particles each)",
+    "plain64": "plain64: 64^3 particles on a 64^3 mesh, L=100 Mpc/h, Zel'dovich field "
+               "P(k)~k^-2 exp(-(0.5k)^2), rms 0.3 spacings",
+}
 FP32_LANES_PER_SM = 128
 # FLOPs charged per evaluated interaction of the walk (the operations of
 # AddPar and AddNode, OST/ost.ver2.c:247-293):
@@ -432,6 +444,134 @@ def run_served(args, E, ic, law, local, dist=None):
     }
 
 
+def fft_check(n, grids, ms_engine, local):
+    """cuFFT (through torch.fft) on the transforms the engine's FFT stage
+    makes: per grid one r2c and one c2r of the n^3 mesh with the Green's
+    function applied between them. Only a check: the engine never calls
+    cuFFT. Timed with CUDA events, best of 5 after 2 warm-ups."""
+    import torch
+    dev = f"cuda:{local}"
+    x = torch.randn((n, n, n), dtype=torch.float32, device=dev)
+    g = torch.rand((n, n, n // 2 + 1), dtype=torch.float32, device=dev)
+
+    def once():
+        for _ in range(grids):
+            torch.fft.irfftn(torch.fft.rfftn(x) * g, s=(n, n, n))
+
+    for _ in range(2):
+        once()
+    best = None
+    for _ in range(5):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        once()
+        b.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b)
+        best = t if best is None else min(best, t)
+    del x, g
+    torch.cuda.empty_cache()
+    return {"ms_engine": ms_engine, "ms_cufft": best, "grids": grids, "mesh": n,
+            "transforms": f"{grids} x (r2c + Green + c2r) of {n}^3 float32",
+            "engine_over_cufft": (ms_engine / best) if (ms_engine and best) else None}
+
+
+def step_roofline(npart, n, grids, counters, ms_step, hbm_gbs, fp32_tflops):
+    """T_roof = minimal HBM bytes of the HBM-bound stages / measured copy
+    bandwidth + walk flops / FP32 peak, against the measured step. Bytes per
+    particle (Np = n^3): sort 28 (12 position read + 12 write + 4
+    permutation), deposit 12 + 4 per grid, FFT 16 per grid (one read and one
+    write per transform), gradient + interpolation 24 + 4 per grid; tree
+    build 12 per particle + 64 per node."""
+    mesh_pp = n ** 3 / npart
+    b = npart * (28 + (12 + 4 * grids * mesh_pp) + 16 * grids * mesh_pp + (24 + 4 * grids * mesh_pp) + 12) + \
+        64 * counters["nodes"]
+    t_hbm = b / (hbm_gbs * 1e9) * 1e3
+    flops = FLOP_PP * counters["pp"] + FLOP_PC * counters["pc"]
+    t_fp32 = flops / (fp32_tflops * 1e12) * 1e3
+    t_roof = t_hbm + t_fp32
+    return {"ms_roofline": t_roof, "ms_hbm_part": t_hbm, "ms_fp32_part": t_fp32, "ms_measured": ms_step,
+            "frac": t_roof / ms_step, "bytes": b, "walk_flops": flops,
+            "peaks": f"HBM {hbm_gbs:.0f} GB/s (measured copy), FP32 {fp32_tflops:.1f} TFLOP/s (nominal)"}
+
+
+def run_clustered(args, E, ic, local, dist=None):
+    """The clustered 256^3 workload (200 Plummer spheres) with the headline
+    law: throughput with positions resident in HBM and the error against
+    the FP64 Ewald sum."""
+    import torch
+    ps = ic.workload("clustered256")
+    pu = ps.positions_u32()
+    eng = E.Engine(256, epsilon=EPS, device=local, **HEADLINE_LAW)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    pos_dev = torch.from_numpy(pu.view(np.int32)).to(f"cuda:{local}")
+    f_dev = torch.empty((ps.np, 3), dtype=torch.float32, device=f"cuda:{local}")
+    eng.load_fixed(pos_dev)
+    if not args.no_autotune:
+        eng.autotune(E.TUNE_FFT | E.TUNE_GROUPS)
+    for _ in range(3):
+        eng.compute(E.PART_ALL)
+        eng.forces(f_dev)
+    steps = max(3, min(args.steps, 10))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    stages = {k: 0.0 for k in E.STAGES}
+    a.record(stream)
+    for _ in range(steps):
+        eng.compute(E.PART_ALL)
+        eng.forces(f_dev)
+        st = eng.stage_times()
+        for k in stages:
+            stages[k] += st.get(k, 0.0)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    out = {"workload": WORKLOADS["clustered256"], "law": HEADLINE_LAW, "steps": steps, "ms_per_step": ms,
+           "value": ps.np / (ms * 1e-3) / 1e6, "unit": UNIT,
+           "stage_ms": {k: v / steps for k, v in stages.items()}, "counters": eng.counters()}
+    if not args.no_ewald:
+        rng = np.random.Generator(np.random.PCG64(4096))
+        tg = np.sort(rng.choice(ps.np, 4096, replace=False)).astype(np.int64)
+        few = eng.ewald(tg)
+        fh = f_dev.cpu().numpy()
+        e = np.linalg.norm(fh[tg].astype(np.float64) - few, axis=1) / np.linalg.norm(few, axis=1)
+        out["err_vs_ewald"] = {"rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)),
+                               "targets": 4096}
+    eng.close()
+    del pos_dev, f_dev
+    torch.cuda.empty_cache()
+    return out
+
+
+def parity_vs_reference(E, local):
+    """The engine with the reference's law on the CPU sample (clustered 128^3)
+    against the reference's own pmmain + treecorrection built from its
+    sources (variant B, the three one-line fixes): per-particle relative
+    force error, every particle."""
+    from oracle import oracle as O
+    if not O.ref_available(O.VARIANT_B):
+        return {"unavailable": "oracle/_ref/libref_B.so was not built"}
+    ps = reference_sample()
+    with E.Engine(ps.n_mesh, epsilon=EPS, device=local, **REFERENCE_LAW) as eng:
+        eng.load_fixed(ps.positions_u32())
+        eng.compute(E.PART_ALL)
+        f = eng.forces()
+    saved = _quiet_stdout()
+    try:
+        fr = O.ref_pm_force(ps.n_mesh, ps.indx, ps.offset, 0.9).astype(np.float64) + \
+            O.ref_tree_force(ps.n_mesh, ps.indx, ps.offset, theta=0.3, rsphere=4.0, eps=EPS, variant=O.VARIANT_B)
+    finally:
+        _restore_stdout(saved)
+    e = O.rel_err(f, fr)
+    return {"sample": f"clustered workload at 128^3, {ps.np} particles, reference law (theta 0.3, rsphere 4)",
+            "oracle": "reference pmmain + treecorrection built from its sources (variant B)",
+            "rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)), "particles": ps.np}
+
+
 def run_engine_arm(args):
     import torch
     from lageunha_b200 import engine as E
@@ -628,9 +768,10 @@ def run_engine_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded Zel'dovich field + Plummer spheres; no dataset)",
-        "config": {"workload": args.workload + (f" at {n}^3" if args.scale else "") +
-                               " (one TreePM force evaluation per step, plain engine)",
+        "data": "synthetic (seeded Zel'dovich field" + (" + Plummer spheres" if args.workload == "clustered256" else "")
+                + "; no dataset)",
+        "config": {"workload": WORKLOADS[args.workload] + (f", at {n}^3" if args.scale else "") +
+                               "; one TreePM force evaluation per step, plain engine",
                    "n_mesh": n, "particles_per_gpu": npart, "epsilon": EPS, **law,
                    "l2": f"inputs larger than L2: {12 * npart / 1e6:.0f} MB of positions, "
                          f"{4 * n ** 3 / 1e6:.0f} MB mesh",
@@ -652,6 +793,11 @@ def run_engine_arm(args):
         "clocks": {"sm_mhz": clocks.get("sm_mhz"), "sm_max_mhz": clocks.get("sm_max_mhz"),
                    "reasons": clocks.get("reasons", [])},
     }
+    # ---- cuFFT on the same transforms, as a check of the hand-written FFT
+    line["fft_check"] = fft_check(n, grids, per.get("fft"), local)
+    # ---- the whole step against its roofline: the HBM time of the stages'
+    # minimal bytes plus the FP32 time of the walk's counted flops
+    line["step_roofline"] = step_roofline(npart, n, grids, counters, ms_step, hbm_peak, fp32_peak)
     # ---- KDK global steps of the same box (drag, forces, kicks, drift),
     # velocities of the workload, anow from 5; the step is sized so that the
     # first drift moves particles by 0.05 cells rms (0.02 for a cold start)
@@ -681,6 +827,10 @@ def run_engine_arm(args):
         ek = np.linalg.norm(fk[tg].astype(np.float64) - fe, axis=1) / np.linalg.norm(fe, axis=1)
         line["kdk"]["err_vs_ewald"] = {"rms": float(np.sqrt(np.mean(ek * ek))), "p99": float(np.percentile(ek, 99))}
     eng.close()
+    del pos_dev, f_dev, vel_dev
+    torch.cuda.empty_cache()
+    if args.workload != "clustered256" and not args.no_clustered:
+        line["clustered256"] = run_clustered(args, E, ic, local, dist)
     if not args.no_ic:
         line["ic"] = run_ic(E, ic, n, local)
     box_law = REFERENCE_LAW if args.law == "reference" else BOX_LAW
@@ -690,6 +840,7 @@ def run_engine_arm(args):
         line["served"] = {"law": box_law, **run_served(args, E, ic, box_law, local, dist)}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+        line["parity_vs_reference"] = parity_vs_reference(E, local)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
@@ -704,7 +855,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", default="clustered256", choices=["clustered256", "plain64", "scale512"])
+    ap.add_argument("--workload", default="scale512", choices=["clustered256", "plain64", "scale512"])
     ap.add_argument("--scale", type=int, default=None,
                     help="mesh size of a smaller instance of the workload (profiling captures)")
     ap.add_argument("--law", default="gaussian", choices=["gaussian", "reference"],
@@ -717,11 +868,15 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the served request-loop block")
     ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--served-requests", type=int, default=32)
-    ap.add_argument("--kdk-steps", type=int, default=1, help="timed KDK global steps of the workload")
+    ap.add_argument("--kdk-steps", type=int, default=None,
+                    help="timed KDK global steps of the workload (default: 10 at scale, else 1)")
+    ap.add_argument("--no-clustered", action="store_true", help="skip the clustered 256^3 block")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in launch shapes")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.kdk_steps is None:
+        args.kdk_steps = 10 if args.workload == "scale512" else 1
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_engine_arm(args)
