@@ -205,7 +205,8 @@ def cpu_baseline():
     return {"value": ps.np / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
             "sample": f"clustered workload at 128^3 ({ps.np} particles, 25 Plummer spheres), one "
                       f"pmmain + treecorrection of the reference built from its sources (variant A), "
-                      f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s",
+                      f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s; its FFTs run on the harness's "
+                      f"double-precision DFT (oracle/dft.c) in place of FFTW, which is not built",
             "ic_reference": reference_ic_time(128)}
 
 
@@ -254,7 +255,8 @@ def run_reference_arm(args):
         "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                          "sample": f"{ps.np} particles (clustered 128^3) per step, reference pmmain + "
-                                   f"treecorrection (variant A) on {os.cpu_count()} host threads"},
+                                   f"treecorrection (variant A) on {os.cpu_count()} host threads; FFTs on "
+                                   f"the harness's double-precision DFT (oracle/dft.c), not FFTW"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -257,6 +257,10 @@ static void free_mesh(tpm_ctx *c) {
   if (c->phi) cudaFree(c->phi);
   if (c->tile_start) cudaFree(c->tile_start);
   if (c->cube_start) cudaFree(c->cube_start);
+  if (c->tb.cube_node) cudaFree(c->tb.cube_node);
+  if (c->tb.start_cube) cudaFree(c->tb.start_cube);
+  c->tb.cube_node = c->tb.start_cube = nullptr;
+  c->tb.ncubes4 = 0;
   fft_plan_free(c->fp);
   c->rho = nullptr;
   c->spec = nullptr;
@@ -280,6 +284,9 @@ static int alloc_mesh(tpm_ctx *c) {
   CK(cudaMalloc(&c->tile_start, sizeof(uint32_t) * (ntiles + 1)));
   c->ncubes = 1ll << (3 * (g.cbits - 2));
   CK(cudaMalloc(&c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
+  c->tb.ncubes4 = c->ncubes;
+  CK(cudaMalloc(&c->tb.cube_node, sizeof(uint32_t) * c->ncubes));
+  CK(cudaMalloc(&c->tb.start_cube, sizeof(uint32_t) * (c->ncubes + 1)));
   fft_plan_init(c->fp, g.n, c->st);
   if (make_phi_tensor_map(g, c->phi, 2, &c->tmap2) != 0 || make_phi_tensor_map(g, c->phi, 4, &c->tmap4) != 0)
     return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
@@ -500,7 +507,7 @@ int64_t tpm::ctx_bytes(int n_mesh, int64_t np) {
   // both grids of the interlaced pair (the Gaussian law's second grid)
   int64_t mesh = 2 * (4 * n3 + 8 * g.spec_elems + 4 * (int64_t)g.px * g.py * g.pz) + 4 * g.spec_elems;
   int64_t ntiles = 1ll << (3 * (g.cbits - 3)), ncubes = 1ll << (3 * (g.cbits - 2));
-  mesh += 4 * (ntiles + 1) + 4 * (ncubes + 1) + 8 * (int64_t)(n_mesh + n_mesh / 2 + 1);
+  mesh += 4 * (ntiles + 1) + 3 * 4 * (ncubes + 1) + 8 * (int64_t)(n_mesh + n_mesh / 2 + 1);
   int64_t parts = np * (12 + 12 + 8 + 8 + 4 + 4 + 12 + 12 + 12 + 12) + 4 * 256 * (sort_tiles(np) + 1) + 1024;
   int64_t cap_nodes = np + np / 4 + 64;
   int64_t tree = cap_nodes * (4 + 4 + 4 + 4 + 1 + 16 + 3 * 16 + 32 + 16);

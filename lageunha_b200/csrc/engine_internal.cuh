@@ -112,8 +112,14 @@ struct WalkBox {
   const uint32_t *ngroups;  // device word: the box's group count
   float *ftree;
   uint32_t *err;
+  // where each group's walk starts: the 4-cell cubes of the tree's level
+  // cbits - 2 (2^start_bits per axis, Morton-indexed): the node of a cube, or
+  // kNoNode, and the sorted particle range of every cube
+  const uint32_t *cube_node, *start_cube;
   float cpu, mass, inv_ll;
+  int n_cells, start_bits;
 };
+constexpr uint32_t kNoNode = 0xffffffffu;
 struct TreeBuffers {
   int64_t cap_nodes = 0;
   uint32_t *start = nullptr, *count = nullptr, *child = nullptr, *nchild = nullptr;
@@ -136,6 +142,12 @@ struct TreeBuffers {
   uint32_t *stack = nullptr;        // per-warp global stacks
   int64_t stack_words = 0;
   WalkBox *walkbox = nullptr;       // device copy of this box's walk record
+  // the walk's start tables over the 4-cell cubes (mesh-sized, allocated
+  // with the mesh): node of each cube at tree level cbits - 2 or kNoNode, and
+  // the first sorted particle of each cube (ncubes4 + 1 entries)
+  uint32_t *cube_node = nullptr;
+  uint32_t *start_cube = nullptr;
+  int64_t ncubes4 = 0;
 };
 
 struct TreeParams {

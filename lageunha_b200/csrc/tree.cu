@@ -353,6 +353,14 @@ __global__ void __launch_bounds__(256) k_tree_moments(const uint32_t *__restrict
   }
 }
 
+// The walk's start table: the node of every 4-cell cube at tree level
+// cbits - 2 (the table was cleared to kNoNode before).
+__global__ void k_cube_nodes(const uint64_t *__restrict__ key, TreeBuffers tb, int lev, int shift) {
+  uint32_t b = tb.level_range[2 * lev], e = tb.level_range[2 * lev + 1];
+  for (uint32_t node = b + blockIdx.x * blockDim.x + threadIdx.x; node < e; node += gridDim.x * blockDim.x)
+    tb.cube_node[key[tb.start[node]] >> shift] = node;
+}
+
 void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos, int64_t np,
                 TreeBuffers &tb, uint32_t *err, cudaStream_t st, int64_t *launches) {
   k_tree_root<<<1, 32, 0, st>>>(np, tb, tp.n, tp.sub_bits);
@@ -369,6 +377,13 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
     k_tree_moments<<<kBuildGrid, 256, 0, st>>>(spos, tb, l, tp.cell_per_unit, tp.mass, inv_theta2);
     nl++;
   }
+  // the walk's start tables over the 4-cell cubes
+  const int cbits = kAxisBits - tp.sub_bits;
+  const int shift = 3 * (tp.sub_bits + 2);
+  launch_range_table(key, np, shift, (uint32_t)tb.ncubes4, tb.start_cube, st);
+  cudaMemsetAsync(tb.cube_node, 0xff, sizeof(uint32_t) * tb.ncubes4, st);
+  k_cube_nodes<<<kBuildGrid, 256, 0, st>>>(key, tb, cbits - 2, shift);
+  nl += 3;
   if (launches) *launches += nl;
 }
 
@@ -743,6 +758,38 @@ TPM_D void eval_pc(WarpLists &wl, int m_all, const WalkBox &tb, WalkCtx &w, floa
   }
 }
 
+// The 4-cell cubes along one axis of an n-cell periodic box whose cells meet
+// [lo, hi] (cells, unwrapped): run[0..1] = first cube and count of the first
+// run, run[2..3] of the second (empty unless [lo, hi] wraps past n). Both
+// runs together list each cube once; an interval of n cells or more lists
+// every cube.
+TPM_D void axis_runs(float lo, float hi, int n, int run[4]) {
+  const int ncube = (n + 3) >> 2;
+  const float fn = (float)n;
+  run[0] = 0;
+  run[1] = ncube;
+  run[2] = 0;
+  run[3] = 0;
+  if (hi - lo >= fn) return;
+  float lw = lo - fn * floorf(lo / fn);
+  if (lw >= fn) lw = 0.f;
+  if (lw < 0.f) lw = 0.f;
+  float hw = lw + (hi - lo);
+  int a = min((int)(lw * 0.25f), ncube - 1);
+  if (hw < fn) {
+    int b = min((int)(hw * 0.25f), ncube - 1);
+    run[0] = a;
+    run[1] = b - a + 1;
+    return;
+  }
+  int b = min((int)((hw - fn) * 0.25f), ncube - 1);
+  if (b >= a) return;  // the runs meet: every cube
+  run[0] = a;
+  run[1] = ncube - a;
+  run[2] = 0;
+  run[3] = b + 1;
+}
+
 // The walk stack: the first kStackSmem entries in shared memory, the rest in
 // this warp's global region.
 struct WarpStack {
@@ -844,23 +891,84 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
     float rs2_prune = rs2 * 1.0001f + 1e-4f;
     const GroupBox gbox{cx, cy, cz, hx, hy, hz, rs2_prune};
     int top = 0, npcl = 0, nppl = 0;
-    if (lane == 0) stack.put(0, 0u);
-    top = 1;
+    // The walk starts at the 4-cell cubes (tree level cbits - 2) that meet
+    // the group's reach, not at the root: per axis at most two runs of cube
+    // coordinates (the reach wraps around the periodic box at most once),
+    // one cube per lane per pass. A near cube pushes its node, or, when it
+    // has none (its parent held fewer than kLeafMin particles), appends its
+    // particles. Nodes above that level are larger than the reach and would
+    // only be opened.
+    const int ncell = wl.box.n_cells;
+    int srun[3][4];
+    int stotal;
+    {
+      const float reach = sqrtf(rs2_prune) + 0.01f;
+      const float gc[3] = {cx, cy, cz}, gh[3] = {hx, hy, hz};
+      const uint32_t ur[3] = {w.rx, w.ry, w.rz};
+      stotal = 1;
+      for (int a = 0; a < 3; a++) {
+        float ref = __uint2float_rn(ur[a]) * wl.box.cpu;
+        axis_runs(ref + gc[a] - gh[a] - reach, ref + gc[a] + gh[a] + reach, ncell, srun[a]);
+        stotal *= srun[a][1] + srun[a][3];
+      }
+    }
+    int sj = 0;
     __syncwarp();
     bool failed = false;
-    while (top > 0) {
+    while (top > 0 || sj < stotal) {
+      int kind = 0;  // 0 drop, 1 accept (PC), 2 open (push children), 3 particles (PP)
+      uint32_t c0 = 0, nch = 0, ps = 0, pcnt = 0;
+      uint32_t node = 0;
+      niter++;
+      if (sj < stotal) {
+        int j = sj + lane;
+        sj += 32;
+        if (j < stotal) {
+          int nx = srun[0][1] + srun[0][3], ny = srun[1][1] + srun[1][3];
+          int jj[3] = {j % nx, (j / nx) % ny, j / (nx * ny)};
+          const float gc[3] = {cx, cy, cz}, gh[3] = {hx, hy, hz};
+          const uint32_t ur[3] = {w.rx, w.ry, w.rz};
+          uint32_t cc[3];
+          float d2 = 0.f;
+          for (int a = 0; a < 3; a++) {
+            int c = jj[a] < srun[a][1] ? srun[a][0] + jj[a] : srun[a][2] + (jj[a] - srun[a][1]);
+            cc[a] = (uint32_t)c;
+            // the cube's cells [4c, min(4c + 4, n)) against the group box,
+            // minimum image
+            float c_lo = (float)(4 * c), c_hi = (float)min(4 * c + 4, ncell);
+            float ref = __uint2float_rn(ur[a]) * wl.box.cpu;
+            float d = 0.5f * (c_lo + c_hi) - (ref + gc[a]);
+            d -= (float)ncell * rintf(d / (float)ncell);
+            float e = fmaxf(fabsf(d) - 0.5f * (c_hi - c_lo) - gh[a], 0.f);
+            d2 += e * e;
+          }
+          nvisit++;
+          if (d2 <= rs2_prune) {
+            uint64_t cid = morton3(cc[0], cc[1], cc[2]);
+            uint32_t nd = wl.box.cube_node[cid];
+            if (nd != kNoNode) {
+              kind = 2;
+              c0 = nd;
+              nch = 1;
+            } else {
+              uint32_t s0 = wl.box.start_cube[cid], s1 = wl.box.start_cube[cid + 1];
+              if (s1 > s0) {
+                kind = 3;
+                ps = s0;
+                pcnt = s1 - s0;
+              }
+            }
+          }
+        }
+      } else {
       // narrower pops keep a deep frontier from growing further
       int take = min(top, top > kStackSmem / 2 ? 8 : 32);
-      niter++;
       nvisit += (unsigned long long)take;
-      uint32_t node = 0;
       bool has = lane < take;
       if (has) node = stack.get(top - take + lane);
       __syncwarp();
       top -= take;
       // classify: one 32-byte and one 16-byte record per node
-      int kind = 0;  // 0 drop, 1 accept (PC), 2 open (push children), 3 particles (PP)
-      uint32_t c0 = 0, nch = 0, ps = 0, pcnt = 0;
       if (has) {
         uint4 geo = wl.box.walkA[2 * (int64_t)node];
         uint4 com = wl.box.walkA[2 * (int64_t)node + 1];
@@ -894,6 +1002,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
             }
           }
         }
+      }
       }
       // children to push (at most 8 per lane) and particles to append: one
       // inclusive scan of both, packed as push | cnt << 9 (the push sum is at
@@ -1036,9 +1145,13 @@ WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &
   b.ngroups = tb.counters;  // counters[0] = the group count tree_groups wrote
   b.ftree = ftree;
   b.err = err;
+  b.cube_node = tb.cube_node;
+  b.start_cube = tb.start_cube;
   b.cpu = tp.cell_per_unit;
   b.mass = tp.mass;
   b.inv_ll = (float)(1.0 / ((double)tp.n * (double)tp.n));
+  b.n_cells = (int)tp.n;
+  b.start_bits = kAxisBits - tp.sub_bits - 2;
   return b;
 }
 

@@ -46,3 +46,56 @@ def test_packed_scan_random_lanes():
         push = np.where(kind == 2, rng.integers(1, 9, size=32), 0).astype(np.uint32)
         cnt = np.where(kind == 3, rng.integers(1, 1 << 18, size=32), 0).astype(np.uint32)
         _check(push, cnt)
+
+
+# ------------------------------------------------------------ start cubes
+# The walk starts at the 4-cell cubes that meet a group's reach: per axis the
+# interval [lo, hi] (cells, unwrapped) becomes at most two runs of wrapped
+# cube coordinates (axis_runs in tree.cu, restated here in float32 the way
+# the device computes it). The runs must list every cube whose cells meet the
+# interval modulo n, each once, for meshes that are and are not multiples of
+# four (the last cube of an n = 45 mesh holds one cell).
+def _axis_runs(lo, hi, n):
+    f32 = np.float32
+    lo, hi = f32(lo), f32(hi)
+    ncube = (n + 3) >> 2
+    fn = f32(n)
+    if f32(hi - lo) >= fn:
+        return [(0, ncube)]
+    lw = f32(lo - fn * np.floor(f32(lo / fn)))
+    if lw >= fn or lw < 0:
+        lw = f32(0)
+    hw = f32(lw + f32(hi - lo))
+    a = min(int(lw * f32(0.25)), ncube - 1)
+    if hw < fn:
+        b = min(int(hw * f32(0.25)), ncube - 1)
+        return [(a, b - a + 1)]
+    b = min(int(f32(hw - fn) * f32(0.25)), ncube - 1)
+    if b >= a:
+        return [(0, ncube)]
+    return [(a, ncube - a), (0, b + 1)]
+
+
+def _cubes_meeting(lo, hi, n):
+    ncube = (n + 3) >> 2
+    out = set()
+    for c in range(ncube):
+        c_lo, c_hi = 4 * c, min(4 * c + 4, n)
+        for k in range(int(np.floor(lo / n)) - 1, int(np.floor(hi / n)) + 2):
+            if c_lo + k * n <= hi and c_hi + k * n > lo:
+                out.add(c)
+    return out
+
+
+def test_start_cube_runs_cover_the_reach_once():
+    rng = np.random.default_rng(23)
+    for n in (16, 32, 45, 48, 81, 125, 128, 512):
+        for _ in range(400):
+            centre = rng.uniform(-1.0, n + 1.0)
+            half = rng.uniform(0.0, 4.0) + 3.51
+            lo, hi = centre - half, centre + half
+            runs = _axis_runs(lo, hi, n)
+            listed = [r0 + j for r0, cnt in runs for j in range(cnt)]
+            assert len(listed) == len(set(listed)), (n, lo, hi, runs)
+            assert set(listed) >= _cubes_meeting(lo, hi, n), (n, lo, hi, runs)
+            assert all(0 <= c < (n + 3) >> 2 for c in listed)
