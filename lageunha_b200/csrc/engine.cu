@@ -160,6 +160,11 @@ static int build_law(tpm_ctx *c) {
       tlog[k] = make_float2((float)(v[k] - d), (float)d);
     }
     tlog[kLogEntries] = make_float2(0.f, 0.f);
+    // the first entry from which the column is zero: the walk reads no entry
+    // at or beyond it (the values there are zero anyway)
+    int k0 = kLogEntries;
+    while (k0 > 0 && v[k0 - 1] == 0.0) k0--;
+    c->law.cut_bits = (uint32_t)(kLogBase + k0) << kLogShift;
   }
   // the node terms' derivative columns (Model4TreeForce.c:48-91:
   // -(f'r - f)/(2 r^3) and -(f''r^2 - 3f'r + 3f)/(2 r^5), central

@@ -192,6 +192,10 @@ struct LawTable {
   // 1: the walk tests r <= rsphere per pair (the reference's cut);
   // 0: tlog is zero from the cut on, so the pair test is not needed
   int hard_cut = 1;
+  // without hard_cut: the float bits of s = r^2 + kLogR2Floor from which
+  // every entry of tlog is zero ((kLogBase + k0) << kLogShift, k0 the first
+  // zero entry)
+  uint32_t cut_bits = 0xffffffffu;
 };
 WalkBox walk_box(const TreeParams &tp, const uint32_t *spos, const TreeBuffers &tb, float *ftree,
                  uint32_t *err);

@@ -19,6 +19,7 @@
 // per-target rsphere cuts. Positions are uint32 fixed point; all relative
 // coordinates are exact minimum-image differences converted to float.
 #include <stdio.h>
+#include <string.h>
 
 #include <algorithm>
 
@@ -553,6 +554,21 @@ TPM_D float law_at(float s, uint32_t tlb) {
   return fmaf(c.y, m, c.x);
 }
 
+// The law at s with every pair beyond the cut reading one shared entry: the
+// bin index is clamped at kcut (the first bin from which the Gaussian law's
+// table is zero; for the reference law the bin of rsphere^2, whose value the
+// per-pair test then discards), so the lanes with such pairs all load one
+// address, a broadcast, and the warp's gather spreads over the banks of the
+// pairs inside the cut only. Same value as law_at with the cut applied.
+TPM_D float law_clamped(float s, uint32_t tlb, uint32_t kcut) {
+  uint32_t bits = __float_as_uint(s);
+  uint32_t kk = min(bits >> kLogShift, kcut);
+  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
+  float2 c;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
+  return fmaf(c.y, m, c.x);
+}
+
 // One source against this lane's target: the reference's AddPar
 // (OST/ost.ver2.c:279-293) without the mass factor. The source comes negated
 // (nsx = -x), so dx = tx + nsx is the IEEE difference tx - x. The target
@@ -561,11 +577,11 @@ TPM_D float law_at(float s, uint32_t tlb) {
 // (a cut 2^-20 cells^2 inside r^2 <= rsphere^2); the Gaussian law's table is
 // zero from the cut on and needs no test.
 template <bool kHardCut>
-TPM_D void pp_one(float nsx, float nsy, float nsz, const WalkCtx &w, float rs2, uint32_t tlb, float &ax,
-                  float &ay, float &az) {
+TPM_D void pp_one(float nsx, float nsy, float nsz, const WalkCtx &w, float rs2, uint32_t kcut, uint32_t tlb,
+                  float &ax, float &ay, float &az) {
   float dx = w.tx + nsx, dy = w.ty + nsy, dz = w.tz + nsz;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, kLogR2Floor)));
-  float f = law_at(r2, tlb);
+  float f = law_clamped(r2, tlb, kcut);
   if (kHardCut) f = r2 <= rs2 ? f : 0.f;
   ax = fmaf(dx, f, ax);
   ay = fmaf(dy, f, ay);
@@ -577,11 +593,11 @@ TPM_D void pp_one(float nsx, float nsy, float nsz, const WalkCtx &w, float rs2, 
 // pairs): each half is the IEEE fp32 operation pp_one does, in the same
 // order, so the sums are the same bits as two pp_one calls into the halves.
 template <bool kHardCut>
-TPM_D void pp_two(float2 nsx, float2 nsy, float2 nsz, float2 tx, float2 ty, float2 tz, float rs2, uint32_t tlb,
-                  float2 &ax, float2 &ay, float2 &az) {
+TPM_D void pp_two(float2 nsx, float2 nsy, float2 nsz, float2 tx, float2 ty, float2 tz, float rs2, uint32_t kcut,
+                  uint32_t tlb, float2 &ax, float2 &ay, float2 &az) {
   float2 dx = __fadd2_rn(tx, nsx), dy = __fadd2_rn(ty, nsy), dz = __fadd2_rn(tz, nsz);
   float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(kLogR2Floor, kLogR2Floor))));
-  float2 f = make_float2(law_at(r2.x, tlb), law_at(r2.y, tlb));
+  float2 f = make_float2(law_clamped(r2.x, tlb, kcut), law_clamped(r2.y, tlb, kcut));
   if (kHardCut) {
     f.x = r2.x <= rs2 ? f.x : 0.f;
     f.y = r2.y <= rs2 ? f.y : 0.f;
@@ -607,7 +623,8 @@ struct GroupBox {
 // two packed pairs), sources j, j+1, j+2, j+3 into accumulator sets 0-3.
 template <bool kHardCut>
 TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, WalkCtx &w, float cpu,
-                   const GroupBox &gb, float rs2, const float2 *__restrict__ tl, unsigned long long &npp) {
+                   const GroupBox &gb, float rs2, uint32_t kcut, const float2 *__restrict__ tl,
+                   unsigned long long &npp) {
   int lane = threadIdx.x & 31;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
   float *nsx = reinterpret_cast<float *>(wl.stage);
@@ -665,16 +682,16 @@ TPM_D void eval_pp(WarpLists &wl, int m, const uint32_t *__restrict__ spos, Walk
       float4 xn = *reinterpret_cast<const float4 *>(nsx + j + 4);
       float4 yn = *reinterpret_cast<const float4 *>(nsy + j + 4);
       float4 zn = *reinterpret_cast<const float4 *>(nsz + j + 4);
-      pp_two<kHardCut>(make_float2(x.x, x.y), make_float2(y.x, y.y), make_float2(z.x, z.y), tx, ty, tz, rs2, tlb,
+      pp_two<kHardCut>(make_float2(x.x, x.y), make_float2(y.x, y.y), make_float2(z.x, z.y), tx, ty, tz, rs2, kcut, tlb,
                        a01x, a01y, a01z);
-      pp_two<kHardCut>(make_float2(x.z, x.w), make_float2(y.z, y.w), make_float2(z.z, z.w), tx, ty, tz, rs2, tlb,
+      pp_two<kHardCut>(make_float2(x.z, x.w), make_float2(y.z, y.w), make_float2(z.z, z.w), tx, ty, tz, rs2, kcut, tlb,
                        a23x, a23y, a23z);
       x = xn;
       y = yn;
       z = zn;
     }
   }
-  for (; j < m; j++) pp_one<kHardCut>(nsx[j], nsy[j], nsz[j], w, rs2, tlb, a01x.x, a01y.x, a01z.x);
+  for (; j < m; j++) pp_one<kHardCut>(nsx[j], nsy[j], nsz[j], w, rs2, kcut, tlb, a01x.x, a01y.x, a01z.x);
   if (w.active) {
     w.ax += (a01x.x + a01x.y) + (a23x.x + a23x.y);
     w.ay += (a01y.x + a01y.y) + (a23y.x + a23y.y);
@@ -812,7 +829,7 @@ template <bool kHardCut>
 __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
     const WalkBox *__restrict__ boxes, const uint32_t *__restrict__ gprefix, int nbox,
     uint32_t *__restrict__ gnext, uint32_t *__restrict__ stack_base, uint32_t *__restrict__ stats,
-    const float2 *__restrict__ glog, const float4 *__restrict__ gpc, float rs2) {
+    const float2 *__restrict__ glog, const float4 *__restrict__ gpc, float rs2, uint32_t kcut) {
   extern __shared__ float4 smem4[];
   float2 *tl = reinterpret_cast<float2 *>(smem4);
   float4 *tq = smem4 + kLogSmemF4;
@@ -1070,7 +1087,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
         done += chunk;
         __syncwarp();
         if (nppl == kPpBatch) {
-          eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, tl, npp);
+          eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, kcut, tl, npp);
           nppl = 0;
         }
       }
@@ -1080,7 +1097,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
       continue;
     }
     if (npcl > 0) eval_pc(wl, npcl, wl.box, w, wl.box.cpu, rs2, tl, tq, npc);
-    if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, tl, npp);
+    if (nppl > 0) eval_pp<kHardCut>(wl, nppl, wl.box.spos, w, wl.box.cpu, gbox, rs2, kcut, tl, npp);
     if (w.active) {
       // the tables are per unit LL: this box's 1/N^2
       int64_t i = (int64_t)gs + lane;
@@ -1161,12 +1178,24 @@ static void launch_walk(const WalkBox *boxes, const uint32_t *gprefix, int nbox,
   int grid = walk_grid(smem);
   int64_t max_grid = stack_words / ((int64_t)kWalkWarps * (kStackCap - kStackSmem));
   if (grid > max_grid) grid = (int)max_grid;
+  const float rs2 = rsphere * rsphere;
+  // the bin every pair beyond the cut reads: for the reference law the bin
+  // of rsphere^2 (the per-pair test discards its value), for the Gaussian law
+  // the first bin of the table's zero tail
+  uint32_t kcut;
+  if (law.hard_cut) {
+    uint32_t b;
+    memcpy(&b, &rs2, 4);
+    kcut = b >> kLogShift;
+  } else {
+    kcut = law.cut_bits >> kLogShift;
+  }
   if (law.hard_cut)
     k_tree_walk<true><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.tlog, law.tpc,
-                                                        rsphere * rsphere);
+                                                        rs2, kcut);
   else
     k_tree_walk<false><<<grid, kWalkThreads, smem, st>>>(boxes, gprefix, nbox, gnext, stack, stats, law.tlog,
-                                                         law.tpc, rsphere * rsphere);
+                                                         law.tpc, rs2, kcut);
 }
 
 __global__ void k_set_walkbox(WalkBox *dst, WalkBox v) {
