@@ -98,10 +98,17 @@ TPM_D void tsc_axis3(uint32_t u, uint32_t n, uint32_t half, float scale, float w
   near = a.near;
 }
 
+// The tile accumulates in 32-bit fixed point (integer shared-memory atomics
+// are single operations; float ones are not): weights carry the tile's scale
+// 2^e, the largest power of two for which no node can exceed 2^32 - a node's
+// mass is at most count * mass * 0.75^3 - and the flush multiplies by 2^-e,
+// exactly. Integer sums do not depend on the order of the additions.
+TPM_D void fix_add(uint32_t *acc, int i, float v) { atomicAdd(&acc[i], __float2uint_rn(v)); }
+
 // Adds the 27 weights of every valid lane to acc, merging runs of lanes with
 // the same home node by a warp segmented sum first (dense clumps put many
 // particles on one node).
-TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], const float wy[3],
+TPM_D void deposit_lanes(uint32_t *acc, bool valid, int home, const float wx[3], const float wy[3],
                          const float wz[3], int lane) {
   int key = valid ? home : -1 - lane;
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -112,7 +119,7 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
       for (int c = 0; c < 3; c++)
         for (int b = 0; b < 3; b++)
           for (int a = 0; a < 3; a++)
-            atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], wx[a] * wy[b] * wz[c]);
+            fix_add(acc, home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1)), wx[a] * wy[b] * wz[c]);
     }
     return;
   }
@@ -148,7 +155,7 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
       for (int b = 0; b < 3; b++)
 #pragma unroll
         for (int a = 0; a < 3; a++)
-          atomicAdd(&acc[home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1))], w[a + 3 * b + 9 * c]);
+          fix_add(acc, home + (a - 1) + kDepNx * ((b - 1) + kDepNy * (c - 1)), w[a + 3 * b + 9 * c]);
   }
 }
 
@@ -156,18 +163,19 @@ TPM_D void deposit_lanes(float *acc, bool valid, int home, const float wx[3], co
 // periodic mesh. vec4: the mesh's x rows are added as float4 groups aligned
 // to 4 cells, [t-4, t), ..., [t+8, t+12), read from the accumulator with
 // the cells outside it as zero.
-TPM_D void flush_tile(const float *acc, float *__restrict__ rho, int n, int ox, int oy, int oz, int vec4, int tid) {
+TPM_D void flush_tile(const uint32_t *acc, float inv_scale, float *__restrict__ rho, int n, int ox, int oy, int oz,
+                      int vec4, int tid) {
   constexpr int kUsed = kTile + 3;  // nodes [t-1, t+9] per axis
   if (vec4) {
     for (int i = tid; i < 4 * kUsed * kUsed; i += kDepThreads) {
       int q = i & 3, r = i >> 2;
       int y = r % kUsed, z = r / kUsed;
-      const float *row = acc + kDepNx * (y + kDepNy * z);
+      const uint32_t *row = acc + kDepNx * (y + kDepNy * z);
       float v[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         int xi = 4 * q - 3 + j;
-        v[j] = (xi >= 0 && xi < kUsed) ? row[xi] : 0.f;
+        v[j] = (xi >= 0 && xi < kUsed) ? (float)row[xi] * inv_scale : 0.f;
       }
       if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f && v[3] == 0.f) continue;
       int gx = ox - 3 + 4 * q, gy = oy + y, gz = oz + z;
@@ -181,7 +189,7 @@ TPM_D void flush_tile(const float *acc, float *__restrict__ rho, int n, int ox, 
     for (int i = tid; i < kUsed * kUsed * kUsed; i += kDepThreads) {
       int x = i % kUsed, r = i / kUsed;
       int y = r % kUsed, z = r / kUsed;
-      float v = acc[x + kDepNx * (y + kDepNy * z)];
+      float v = (float)acc[x + kDepNx * (y + kDepNy * z)] * inv_scale;
       if (v == 0.f) continue;
       int gx = ((ox + x) % n + n) % n, gy = ((oy + y) % n + n) % n, gz = ((oz + z) % n + n) % n;
       atomicAdd(rho + gx + (int64_t)n * (gy + (int64_t)n * gz), v);
@@ -195,7 +203,7 @@ TPM_D void flush_tile(const float *acc, float *__restrict__ rho, int n, int ox, 
 __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
     const uint32_t *__restrict__ spos, const uint32_t *__restrict__ tile_start, int n, int cbits,
     float mass, float *__restrict__ rho, uint32_t half, int vec4) {
-  __shared__ __align__(16) float acc[kDepCells];
+  __shared__ __align__(16) uint32_t acc[kDepCells];
   int tid = threadIdx.x, lane = tid & 31;
   // Morton tile index -> tile coordinates
   uint32_t t = blockIdx.x;
@@ -208,7 +216,13 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
   uint32_t p0 = tile_start[t], p1 = tile_start[t + 1];
   if (p0 == p1) return;
   int ox = (int)tx * kTile - 1, oy = (int)ty * kTile - 1, oz = (int)tz * kTile - 1;
-  for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0.f;
+  for (int i = tid; i < kDepCells; i += kDepThreads) acc[i] = 0u;
+  // fixed-point scale 2^e: count * mass * 0.75^3 * 2^e < 2^31 (a factor two
+  // below the 32-bit limit for the rounding of each contribution)
+  int e;
+  frexpf((float)(p1 - p0) * mass * 0.421875f, &e);
+  e = min(31 - e, 40);
+  const float scale = ldexpf(1.f, e), inv_scale = ldexpf(1.f, -e);
   __syncthreads();
   uint32_t nu = (uint32_t)n;
   int nwarp_items = (int)((p1 - p0 + 31) / 32) * 32;
@@ -234,7 +248,7 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
     int home = 0;
     if (valid) {
       int hx, hy, hz;
-      tsc_axis3(u[0], nu, half, mass, wx, hx);
+      tsc_axis3(u[0], nu, half, mass * scale, wx, hx);
       tsc_axis3(u[1], nu, half, 1.f, wy, hy);
       tsc_axis3(u[2], nu, half, 1.f, wz, hz);
       home = (hx - ox) + kDepNx * ((hy - oy) + kDepNy * (hz - oz));
@@ -242,7 +256,7 @@ __global__ void __launch_bounds__(kDepThreads) k_tsc_deposit(
     deposit_lanes(acc, valid, home, wx, wy, wz, lane);
   }
   __syncthreads();
-  flush_tile(acc, rho, n, ox, oy, oz, vec4, tid);
+  flush_tile(acc, inv_scale, rho, n, ox, oy, oz, vec4, tid);
 }
 
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
@@ -1133,7 +1147,7 @@ TPM_D void fda_load_box(const CUtensorMap *tmap, float *box, uint64_t *bar, int 
 // of kNodes nodes per thread and axis: the line's kNodes + 2R potential
 // values are read once and the differences taken in registers.
 template <int R>
-TPM_D void fda_node_gradients(const float *boxf, float2 *gxy, float *gz) {
+TPM_D void fda_node_gradients(const float *boxf, float *gx, float *gy, float *gz) {
   using B = FdaBox<R>;
   const float(*box)[B::BY][B::BX] = reinterpret_cast<const float(*)[B::BY][B::BX]>(boxf);
   constexpr int kLine = kNodes + 2 * R;
@@ -1165,9 +1179,9 @@ TPM_D void fda_node_gradients(const float *boxf, float2 *gxy, float *gz) {
         f = c1 * (w[-1] - w[1]) + c2 * (w[-2] - w[2]) + c3 * (w[-3] - w[3]) + c4 * (w[-4] - w[4]);
       }
       if (axis == 0)
-        gxy[a + kGradSy * p + kGradSz * q].x = f;
+        gx[a + kGradSy * p + kGradSz * q] = f;
       else if (axis == 1)
-        gxy[p + kGradSy * a + kGradSz * q].y = f;
+        gy[p + kGradSy * a + kGradSz * q] = f;
       else
         gz[p + kGradSy * q + kGradSz * a] = f;
     }
@@ -1178,8 +1192,8 @@ TPM_D void fda_node_gradients(const float *boxf, float2 *gxy, float *gz) {
 // summed in the reference's order wt_n, n = a + 3b + 9c (fda4.h:67-102,
 // 276-292); node indices i1 = near, i2 = near + sign, i3 = near - sign
 // (fda4.h:46-54), relative to the tile's first node t - 1.
-TPM_D float3 fda_interp(const float2 *gxy, const float *gz, uint32_t ux, uint32_t uy, uint32_t uz, uint32_t n,
-                        uint32_t half, int x0, int y0, int z0) {
+TPM_D float3 fda_interp(const float *gx, const float *gy, const float *gz, uint32_t ux, uint32_t uy, uint32_t uz,
+                        uint32_t n, uint32_t half, int x0, int y0, int z0) {
   Axis ax = axis_of(ux, n, half), ay = axis_of(uy, n, half), az = axis_of(uz, n, half);
   float wx1, wx2, wx3, wy1, wy2, wy3, wz1, wz2, wz3;
   int sx, sy, sz;
@@ -1199,9 +1213,8 @@ TPM_D float3 fda_interp(const float2 *gxy, const float *gz, uint32_t ux, uint32_
       for (int a = 0; a < 3; a++) {
         float wt = wab[a] * wzs[c];
         int node = ii[a] + kGradSy * jj[b] + kGradSz * kk[c];
-        float2 g = gxy[node];
-        fx += wt * g.x;
-        fy += wt * g.y;
+        fx += wt * gx[node];
+        fy += wt * gy[node];
         fz += wt * gz[node];
       }
     }
@@ -1222,14 +1235,17 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
                                                       uint32_t *__restrict__ err, uint32_t half, int average) {
   using B = FdaBox<R>;
   // dynamic shared memory: the potential box (128-byte aligned for TMA), then
-  // the gradient at the nodes as {-dphi/dx, -dphi/dy} pairs and -dphi/dz
-  // (twice with kPair)
+  // the gradient at the nodes, -dphi/dx, -dphi/dy and -dphi/dz as three float
+  // arrays (twice with kPair): with the strides 1, 12, 144 the 27 node reads
+  // of 32 Morton-consecutive particles are each one wavefront
   extern __shared__ __align__(128) float fda_smem[];
   float *box = fda_smem;
-  float2 *gxy = reinterpret_cast<float2 *>(fda_smem + B::BY * B::BY * B::BX);
-  float *gz = reinterpret_cast<float *>(gxy + kGradSize);
-  float2 *gxy2 = reinterpret_cast<float2 *>(gz + kGradSize);
-  float *gz2 = reinterpret_cast<float *>(gxy2 + kGradSize);
+  float *gx = fda_smem + B::BY * B::BY * B::BX;
+  float *gy = gx + kGradSize;
+  float *gz = gy + kGradSize;
+  float *gx2 = gz + kGradSize;
+  float *gy2 = gx2 + kGradSize;
+  float *gz2 = gy2 + kGradSize;
   __shared__ __align__(8) uint64_t bar;
   int tid = threadIdx.x;
   uint32_t t = blockIdx.x;
@@ -1257,7 +1273,7 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
       mbar_wait_bounded(&bar, (uint32_t)gi, 1ll << 20);  // let an in-flight copy land before exit
       return;
     }
-    fda_node_gradients<R>(box, gi == 0 ? gxy : gxy2, gi == 0 ? gz : gz2);
+    fda_node_gradients<R>(box, gi == 0 ? gx : gx2, gi == 0 ? gy : gy2, gi == 0 ? gz : gz2);
     __syncthreads();
   }
   uint32_t nu = (uint32_t)n;
@@ -1275,10 +1291,10 @@ __global__ void __launch_bounds__(kFdaThreads) k_fda4(const __grid_constant__ CU
       ny = spos[3 * (int64_t)kn + 1];
       nz = spos[3 * (int64_t)kn + 2];
     }
-    float3 f = fda_interp(gxy, gz, ux, uy, uz, nu, kPair ? 0u : half, x0, y0, z0);
+    float3 f = fda_interp(gx, gy, gz, ux, uy, uz, nu, kPair ? 0u : half, x0, y0, z0);
     if (kPair) {
       // the mean of the two grids' forces
-      float3 f2 = fda_interp(gxy2, gz2, ux, uy, uz, nu, 1u, x0, y0, z0);
+      float3 f2 = fda_interp(gx2, gy2, gz2, ux, uy, uz, nu, 1u, x0, y0, z0);
       f = make_float3(0.5f * (f.x + f2.x), 0.5f * (f.y + f2.y), 0.5f * (f.z + f2.z));
     } else if (average) {
       // the second grid of the interlaced pair: mean of the two grids' forces
