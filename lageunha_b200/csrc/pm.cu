@@ -339,6 +339,23 @@ TPM_D Div make_div(int d) {
   return r;
 }
 
+// Shared-memory slot of element m of a pencil: one spare slot after every 16
+// elements. The first Stockham stage writes at stride R (up to 16 float2, so
+// a half-warp's 16 lanes would hit one bank pair); with the spare slots those
+// writes, and the column passes' transposing loads and stores, fall on
+// distinct bank pairs.
+TPM_HD int fslot(int m) { return m + (m >> 4); }
+// slots a pencil of L elements spans
+TPM_HD int fslots(int L) { return fslot(L - 1) + 1; }
+// Pencil stride of the column passes for P pencils per block: at least
+// fslots(n), and = 16/P (mod 16) for P < 16 (odd for P >= 16), so the P
+// pencils of a transposing load's half-warp start on distinct bank pairs.
+TPM_HD int col_stride(int n, int P) {
+  int s = fslots(n);
+  int r = P >= 16 ? 1 : (16 / P);
+  return s + (((r - s) % 16) + 16) % 16;
+}
+
 TPM_D float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 TPM_D float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 TPM_D float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -462,7 +479,7 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
     float2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      float2 x = src[j + r * jobs_per];
+      float2 x = src[fslot(j + r * jobs_per)];
       if (r) {
         float2 w = tw[r * k * step];  // r k step < L: r < R, k < Ns, step = L / (Ns R)
         if (dir > 0) w.y = -w.y;
@@ -473,11 +490,12 @@ TPM_D void stockham_stage(const float2 *in, float2 *out, const float2 *tw, int L
     dft_small<R>(v, dir);
     int d0 = jn * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) dst[d0 + r * Ns] = v[r];
+    for (int r = 0; r < R; r++) dst[fslot(d0 + r * Ns)] = v[r];
   }
 }
 
-// Transforms P pencils of length L (pencil p at p * ld) from a to scratch b
+// Transforms P pencils of length L (pencil p at p * ld, element m at slot
+// fslot(m), ld >= fslots(L)) from a to scratch b
 // and back as needed; returns the buffer holding the result. dir = -1
 // forward, +1 backward (unnormalised, FFTW sign convention).
 __device__ float2 *fft_pencils(float2 *a, float2 *b, const float2 *tw, int L, int ld, int P, float dir,
@@ -573,10 +591,10 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
                             const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n,
                             int64_t nrows) {
   extern __shared__ float2 sm[];
-  int L = a.L, P = a.P, n = a.n, hx = a.hx;
+  int L = a.L, P = a.P, n = a.n, hx = a.hx, ld = fslots(L);
   float2 *twl = sm;
   float2 *A = sm + L;
-  float2 *B = A + P * L;
+  float2 *B = A + P * ld;
   int tid = threadIdx.x, nth = blockDim.x;
   for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
   int64_t row0 = (int64_t)blockIdx.x * P;
@@ -599,26 +617,31 @@ __global__ void k_fft_x_r2c(const float *__restrict__ rho, float2 *__restrict__ 
       }
     }
 #pragma unroll
-    for (int u = 0; u < kLoadBatch; u++)
-      if (e0 + u * nth < P * L) A[e0 + u * nth] = v[u];
+    for (int u = 0; u < kLoadBatch; u++) {
+      int e = e0 + u * nth;
+      if (e < P * L) {
+        int p = dL.q(e);
+        A[p * ld + fslot(e - p * L)] = v[u];
+      }
+    }
   }
   __syncthreads();
-  float2 *res = fft_pencils(A, B, twl, L, L, P, -1.f, a.radix, a.nf);
+  float2 *res = fft_pencils(A, B, twl, L, ld, P, -1.f, a.radix, a.nf);
   for (int e = tid; e < P * hx; e += nth) {
     int p = dH.q(e), k = e - p * hx;
     int64_t row = row0 + p;
     if (row >= nrows) continue;
     float2 X;
     if (packed) {
-      const float2 *Z = res + p * L;
-      float2 zk = Z[k == L ? 0 : k], zc = cconj(Z[k == 0 ? 0 : L - k]);  // k <= L
+      const float2 *Z = res + p * ld;
+      float2 zk = Z[fslot(k == L ? 0 : k)], zc = cconj(Z[fslot(k == 0 ? 0 : L - k)]);  // k <= L
       float2 ev = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y));
       float2 od = make_float2(0.5f * (zk.x - zc.x), 0.5f * (zk.y - zc.y));  // times -i below
       float2 w = tw_n[k];  // k <= L < n
       float2 wo = cmul(w, make_float2(od.y, -od.x));
       X = cadd(ev, wo);
     } else {
-      X = res[p * L + k];
+      X = res[p * ld + fslot(k)];
     }
     spec[row * hx + k] = X;
   }
@@ -706,7 +729,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
   extern __shared__ float2 sm[];
   // pencils one element apart beyond their length: the transposing loads
   // and stores (consecutive threads on consecutive pencils) hit distinct banks
-  int n = a.n, hx = a.hx, L = n, P = TX * nspec, Lp = n + 1;
+  int n = a.n, hx = a.hx, L = n, P = TX * nspec, Lp = col_stride(n, P);
   float2 *twl = sm;
   float2 *A = sm + L;
   float2 *B = A + P * Lp;
@@ -734,7 +757,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     for (int u = 0; u < kLoadBatch; u++) {
       int e = e0 + u * nth;
       int m = dP.q(e);
-      if (e < P * L) A[(e - m * P) * Lp + m] = v[u];
+      if (e < P * L) A[(e - m * P) * Lp + fslot(m)] = v[u];
     }
   }
   __syncthreads();
@@ -746,7 +769,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     int wy = outer > n / 2 ? outer - n : outer;
     for (int e = tid; e < TX * L; e += nth) {
       int q = dL.q(e), m = e - q * L;
-      if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[q * Lp + m]);
+      if (kx0 + q < hx) pk_accumulate(sbin, n, kx0 + q, wy, m > n / 2 ? m - n : m, res[q * Lp + fslot(m)]);
     }
     __syncthreads();
     for (int e = tid; e < 2 * (n + 1); e += nth)
@@ -757,8 +780,8 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
       for (int e = tid; e < P * L; e += nth) {
         int q = dL.q(e), m = e - q * L;
         float gk = green(ga, kx0 + q, outer, m);
-        float2 v = res[q * Lp + m];
-        res[q * Lp + m] = make_float2(v.x * gk, v.y * gk);
+        float2 v = res[q * Lp + fslot(m)];
+        res[q * Lp + fslot(m)] = make_float2(v.x * gk, v.y * gk);
       }
     } else {
       int wy = outer > n / 2 ? outer - n : outer;
@@ -782,7 +805,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
         if ((n & 1) == 0 && (2 * kx == n || 2 * wy == n || 2 * wz == n || -2 * wy == n || -2 * wz == n)) gk = 0.f;
         float s, c;
         sincospif((float)(kx + wy + wz) / (float)n, &s, &c);
-        int i1 = q * Lp + m, i2 = (q + TX) * Lp + m;
+        int i1 = q * Lp + fslot(m), i2 = (q + TX) * Lp + fslot(m);
         float2 r1 = res[i1], r2 = res[i2];
         // (rho1 + e^{i theta} rho2) / 2, then times G
         float2 rho = make_float2(0.5f * (r1.x + c * r2.x - s * r2.y), 0.5f * (r1.y + c * r2.y + s * r2.x));
@@ -800,7 +823,7 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
     int m = dP.q(e), q = e - m * P;
     int qs = q < TX ? q : q - TX;
     float2 *dst = q < TX ? spec : spec2;
-    if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * Lp + m];
+    if (qs < tw_) dst[base + m * stride + kx0 + qs] = res[q * Lp + fslot(m)];
   }
 }
 
@@ -811,10 +834,10 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
                             const float2 *__restrict__ tw_L, const float2 *__restrict__ tw_n,
                             int64_t nrows, int px, int py) {
   extern __shared__ float2 sm[];
-  int L = a.L, P = a.P, n = a.n, hx = a.hx;
+  int L = a.L, P = a.P, n = a.n, hx = a.hx, ld = fslots(L);
   float2 *twl = sm;
   float2 *A = sm + L;
-  float2 *B = A + P * L;
+  float2 *B = A + P * ld;
   int tid = threadIdx.x, nth = blockDim.x;
   for (int k = tid; k < L; k += nth) twl[k] = tw_L[k];
   int64_t row0 = (int64_t)blockIdx.x * P;
@@ -843,7 +866,7 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
     for (int u = 0; u < kB; u++) {
       int e = e0 + u * nth;
       if (e >= P * L) break;
-      int k = e - dL.q(e) * L;
+      int pk = dL.q(e), k = e - pk * L;
       float2 Zk;
       if (packed) {
         // Z_k = (X_k + conj X_{L-k}) + i conj(W^k) (X_k - conj X_{L-k})
@@ -861,11 +884,11 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
         Zk = k < hx ? xa[u] : cconj(xa[u]);
         if (k == 0) Zk.y = 0.f;
       }
-      A[e] = Zk;
+      A[pk * ld + fslot(k)] = Zk;
     }
   }
   __syncthreads();
-  float2 *res = fft_pencils(A, B, twl, L, L, P, 1.f, a.radix, a.nf);
+  float2 *res = fft_pencils(A, B, twl, L, ld, P, 1.f, a.radix, a.nf);
   // threads run over (pencil, x) pairs of the block's rows, x in
   // [-kGhost, n + kGhost) (n >= 16 > kGhost, so one wrap maps x into [0, n))
   const int W = n + 2 * kGhost;
@@ -896,10 +919,10 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
       int xs = x < 0 ? x + n : (x >= n ? x - n : x);
       float v;
       if (packed) {
-        float2 c = res[p * L + (xs >> 1)];
+        float2 c = res[p * ld + fslot(xs >> 1)];
         v = (xs & 1) ? c.y : c.x;
       } else {
-        v = res[p * L + xs].x;
+        v = res[p * ld + fslot(xs)].x;
       }
       for (int iz = 0; iz < 2; iz++) {
         if (zs[iz] == 0x7fffffff) continue;
@@ -916,7 +939,7 @@ __global__ void k_fft_x_c2r(const float2 *__restrict__ spec, float *__restrict__
 static int pencils_for(int L, int want = 0) {
   if (want > 0) {
     // a tuned count, kept within the 160 KB of shared memory
-    int cap = (int)(((160 * 1024) / (int)sizeof(float2) - L) / (2 * L));
+    int cap = (int)(((160 * 1024) / (int)sizeof(float2) - L) / (2 * fslots(L)));
     return std::max(1, std::min(want, cap));
   }
   int P = 4096 / L;
@@ -931,7 +954,7 @@ static int pencils_for(int L, int want = 0) {
 static int cols_per_block(int n, int hx, int nspec, int want = 0) {
   int TX = want > 0 ? want : (n >= 256 ? 8 : 16);
   // room for the power-spectrum bins (2(n+1) floats) as well
-  int tmax = (int)(((160 * 1024 - 8 * (n + 1)) / (int)sizeof(float2) - n) / (2 * nspec * (n + 1)));
+  int tmax = (int)(((160 * 1024 - 8 * (n + 1)) / (int)sizeof(float2) - n) / (2 * nspec * (fslots(n) + 15)));
   if (TX > tmax) TX = tmax;
   if (TX > hx) TX = hx;
   if (TX < 1) TX = 1;
@@ -1010,7 +1033,7 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   int Px = pencils_for(Lx, want_px);
   FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
   const float2 *twL = packed ? p.tw_half : p.tw;
-  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * fslots(Lx));
   int thx = 256;
   int nspec = rho2 ? 2 : 1;
   k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), thx, smx, st>>>(rho, spec, ax, twL, p.tw, nrows);
@@ -1018,7 +1041,8 @@ void launch_poisson(const MeshGeom &g, const FftPlan &p, const float *rho, float
   // columns
   int TX = cols_per_block(n, g.hx, nspec, want_tx);
   FftArgs ac = fft_args(n, n, TX * nspec, kColRadixMax);
-  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * (n + 1)) + (pk ? sizeof(float) * 2 * (n + 1) : 0);
+  size_t smc = sizeof(float2) * (n + 2 * TX * nspec * col_stride(n, TX * nspec)) +
+               (pk ? sizeof(float) * 2 * (n + 1) : 0);
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   ga.law = law;
@@ -1049,12 +1073,12 @@ void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 
   int Lx = packed ? n / 2 : n;
   int Px = pencils_for(Lx);
   FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
-  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * fslots(Lx));
   k_fft_x_r2c<<<(unsigned)((nrows + Px - 1) / Px), 256, smx, st>>>(real, spec, ax, packed ? p.tw_half : p.tw,
                                                                    p.tw, nrows);
   int TX = cols_per_block(n, g.hx, 1);
   FftArgs ac = fft_args(n, n, TX, kColRadixMax);
-  size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
+  size_t smc = sizeof(float2) * (n + 2 * TX * col_stride(n, TX));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   memset(&ga, 0, sizeof(ga));
@@ -1069,10 +1093,10 @@ void fft_inverse(const MeshGeom &g, const FftPlan &p, float2 *spec, float *phi_p
   int Lx = packed ? n / 2 : n;
   int Px = pencils_for(Lx);
   FftArgs ax = fft_args(n, Lx, Px, kXRadixMax);
-  size_t smx = sizeof(float2) * (Lx + 2 * Px * Lx);
+  size_t smx = sizeof(float2) * (Lx + 2 * Px * fslots(Lx));
   int TX = cols_per_block(n, g.hx, 1);
   FftArgs ac = fft_args(n, n, TX, kColRadixMax);
-  size_t smc = sizeof(float2) * (n + 2 * TX * (n + 1));
+  size_t smc = sizeof(float2) * (n + 2 * TX * col_stride(n, TX));
   int ntx = (g.hx + TX - 1) / TX;
   GreenArgs ga;
   memset(&ga, 0, sizeof(ga));

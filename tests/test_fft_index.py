@@ -121,3 +121,86 @@ def test_c2r_flat_write_covers_the_serial_loop():
             a = _c2r_writes_serial(n, P, row0, nrows, px, py)
             b = _c2r_writes_flat(n, P, row0, nrows, px, py)
             assert a == b, (n, P, row0)
+
+
+# ------------------------------------------------------- padded pencil slots
+# Element m of a pencil lives at shared-memory slot fslot(m) = m + m // 16
+# (one spare slot after every 16 elements, so the first Stockham stage's
+# stride-R writes fall on distinct bank pairs). This restates the Stockham
+# stages of pm.cu (stockham_stage / fft_pencils) over those slots and checks
+# the transform against numpy's FFT for the radix sequences the passes use.
+def _fslot(m):
+    return m + (m >> 4)
+
+
+def _factorize(L, rmax=16):
+    r = []
+    while rmax >= 16 and L % 16 == 0:
+        r.append(16); L //= 16
+    if rmax >= 8 and L % 8 == 0:
+        r.append(8); L //= 8
+    while L % 4 == 0:
+        r.append(4); L //= 4
+    while L % 2 == 0:
+        r.append(2); L //= 2
+    while L % 3 == 0:
+        r.append(3); L //= 3
+    while L % 5 == 0:
+        r.append(5); L //= 5
+    assert L == 1
+    return r
+
+
+def _stockham_padded(x, ld, direction):
+    """x: [P, L] complex; returns the [P, L] transform through buffers of
+    P * ld slots addressed by fslot, stage by stage as the kernel does."""
+    P, L = x.shape
+    tw = np.exp(-2j * np.pi * np.arange(L) / L)
+    a = np.zeros(P * ld, np.complex128)
+    b = np.zeros(P * ld, np.complex128)
+    for p in range(P):
+        a[p * ld + _fslot(np.arange(L))] = x[p]
+    src, dst = a, b
+    Ns = 1
+    for R in _factorize(L):
+        jobs = L // R
+        step = L // (Ns * R)
+        j = np.arange(jobs)
+        jn, k = j // Ns, j % Ns
+        for p in range(P):
+            v = np.stack([src[p * ld + _fslot(j + r * jobs)] for r in range(R)])
+            w = np.stack([tw[(r * k * step) % L] for r in range(R)])
+            if direction > 0:
+                w = np.conj(w)
+            v = v * w
+            # size-R DFT with the pass's sign
+            F = np.exp(direction * 2j * np.pi * np.outer(np.arange(R), np.arange(R)) / R)
+            out = F @ v
+            d0 = jn * Ns * R + k
+            for r in range(R):
+                dst[p * ld + _fslot(d0 + r * Ns)] = out[r]
+        src, dst = dst, src
+        Ns *= R
+    return np.stack([src[p * ld + _fslot(np.arange(L))] for p in range(P)])
+
+
+def test_padded_stockham_matches_numpy():
+    rng = np.random.default_rng(5)
+    for L, P in [(16, 3), (32, 2), (64, 2), (128, 1), (256, 1), (512, 1), (48, 2), (60, 2), (75, 1), (81, 1)]:
+        x = rng.standard_normal((P, L)) + 1j * rng.standard_normal((P, L))
+        for direction in (-1, 1):
+            ld = _fslot(L - 1) + 1 + 3  # any stride at least the slots a pencil spans
+            got = _stockham_padded(x, ld, direction)
+            want = np.fft.fft(x, axis=1) if direction < 0 else np.fft.ifft(x, axis=1) * L
+            assert np.allclose(got, want, atol=1e-9 * L), (L, P, direction)
+
+
+def test_padded_slots_spread_the_first_stage_writes():
+    """In the first stage (Ns = 1) job j writes elements R j + r; for the 16
+    consecutive jobs of a half-warp and each r, the slots fall on 16
+    distinct bank pairs (slot mod 16) for every radix the passes use."""
+    for R in (2, 4, 8, 16):
+        for j0 in range(0, 512 // R, 16):
+            for r in range(R):
+                pairs = {_fslot(R * j + r) % 16 for j in range(j0, j0 + 16)}
+                assert len(pairs) == 16, (R, j0, r)
