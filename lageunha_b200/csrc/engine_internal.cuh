@@ -25,7 +25,7 @@ struct SortScratch {
   int64_t cap_tiles = 0;
 };
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortThreads * kSortItems;
 
 void launch_make_keys(const uint32_t *pos, int64_t np, uint32_t n, int sub_bits, uint64_t *key,

@@ -64,7 +64,7 @@ def test_noalloc_order_matches_engine_twice():
 
 
 def test_noalloc_ragged_and_single_particle():
-    """Counts that are not a multiple of the sort's 4096-particle tile (the
+    """Counts that are not a multiple of the sort's 2048-particle tile (the
     partial last tile), a single particle (the sort returns at once and the
     keys and indices reach the caller's buffers by a copy), and a mesh that
     is not a power of two."""
