@@ -269,12 +269,14 @@ int tpm_set_tuning(tpm_ctx *ctx, const tpm_tuning *tuning);
 
 /* ---- the request loop (served solves) ---- */
 
-/* A worker thread on one device admits requests in arrival order while
- * their device footprint fits under hbm_cap_bytes and in the free HBM, keeps
- * each request's particles, mesh and tree on the device between its steps,
- * and runs the active requests' steps as they become ready, so requests that
- * arrive while others run overlap with them on the device. No counterpart in
- * the reference (a batch MPI job). */
+/* On one device, an admission thread admits requests in arrival order while
+ * their device footprint fits under hbm_cap_bytes and in the free HBM
+ * (context, upload, graph capture), and a launch thread runs the active
+ * requests' steps as they become ready, so requests that arrive while others
+ * run overlap with them on the device. Each request's particles, mesh and
+ * tree stay on the device between its steps, in buffers taken from the
+ * server's device arena. No counterpart in the reference (a batch MPI
+ * job). */
 typedef struct tpm_server tpm_server;
 
 typedef struct tpm_request {
@@ -312,8 +314,17 @@ int tpm_server_info(tpm_server *server, int64_t id, tpm_request_info *out);
 int tpm_server_wait(tpm_server *server, int64_t id, double timeout_s);
 /* [0] done [1] failed [2] peak active [3] peak device bytes [4] contexts
  * created [5] contexts reused [6] contexts evicted [7] deferred admissions;
- * returns the number of words written. */
+ * microseconds the admission thread spent [8] making or re-parameterising
+ * contexts [9] uploading particles [10] capturing graphs [11] reserving
+ * memory; [12] device bytes the server's arena holds; returns the number of
+ * words written (at most 13). */
 int tpm_server_stats(tpm_server *server, int64_t *out, int n);
+/* Claims device memory for the server's contexts now, so that admissions
+ * up to `bytes` (at most the cap) take their buffers without a cudaMalloc.
+ * The server otherwise claims memory in 1 GiB blocks as requests need it;
+ * it keeps what it claimed until tpm_server_destroy. No reference
+ * counterpart: the reference has no request loop. */
+int tpm_server_reserve(tpm_server *server, int64_t bytes);
 /* Finishes every submitted request, then stops the worker. */
 int tpm_server_destroy(tpm_server *server);
 

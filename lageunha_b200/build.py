@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtpm_engine.so")
-SOURCES = ["engine.cu", "sort.cu", "pm.cu", "tree.cu", "ewald.cu", "noalloc.cu", "step.cu", "batch.cu", "server.cu", "tune.cu", "snapshot.cpp", "spectrum.cu", "fof.cu", "ic.cu", "stream.cu"]
+SOURCES = ["engine.cu", "arena.cu", "sort.cu", "pm.cu", "tree.cu", "ewald.cu", "noalloc.cu", "step.cu", "batch.cu", "server.cu", "tune.cu", "snapshot.cpp", "spectrum.cu", "fof.cu", "ic.cu", "stream.cu"]
 HEADERS = ["common.cuh", "engine_internal.cuh", "ctx.cuh"]
 
 NVCC_FLAGS = [

@@ -108,6 +108,9 @@ struct tpm_ctx {
   uint32_t *herr = nullptr;  // pinned [8]
   double *hfac = nullptr;    // pinned [kFacWords]
   double *dfac = nullptr;    // device [kFacWords]
+  // where the device buffers come from: the request loop's arena, or
+  // cudaMalloc (nullptr)
+  tpm::DeviceArena *arena = nullptr;
   // bookkeeping
   unsigned parts_valid = 0;
   float stage_ms[tpm::kNStages];
@@ -156,6 +159,10 @@ int launch_finish_to(tpm_ctx *c, cudaStream_t st, unsigned parts, float *out);
 void free_stream_state(tpm_ctx *c);
 // Device bytes a context of this mesh and particle capacity allocates.
 int64_t ctx_bytes(int n_mesh, int64_t np);
+// tpm_create with the context's device buffers taken from an arena (nullptr:
+// cudaMalloc). A context in an arena must not join an ensemble: it drains
+// only its own streams before it releases a buffer.
+int create_ctx(const tpm_params *params, int device, DeviceArena *arena, tpm_ctx **out);
 // Parameter validation of tpm_create / tpm_set_params (sets the error).
 int check_params(const tpm_params *p);
 // The reference's opening-angle schedule (Cosmos/globalT.c:41-44).

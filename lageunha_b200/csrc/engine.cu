@@ -121,6 +121,17 @@ static double law_f(int kind, double r, float eps, double rs, double LL) {
   return (soft - longr) / LL;
 }
 
+// cudaFree waits for the whole device before it returns memory; a range of
+// the context's arena can go to another context at once, so a context in an
+// arena drains its own streams before it releases a buffer.
+static void quiesce(tpm_ctx *c) {
+  if (!c->arena) return;
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->st_pm) cudaStreamSynchronize(c->st_pm);
+  if (c->sp.in) cudaStreamSynchronize(c->sp.in);
+  if (c->sp.out) cudaStreamSynchronize(c->sp.out);
+}
+
 static int build_law(tpm_ctx *c) {
   const tpm_params &p = c->prm;
   if (c->law.tlog && c->law_n == p.n_mesh && c->law_eps == p.epsilon && c->law_kind == p.law &&
@@ -192,14 +203,17 @@ static int build_law(tpm_ctx *c) {
     }
     tpc[kPcEntries] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  if (c->law.tlog || c->law.tpc) CK(cudaStreamSynchronize(c->st));
-  if (c->law.tlog) cudaFree(c->law.tlog);
-  if (c->law.tpc) cudaFree(c->law.tpc);
+  if (c->law.tlog || c->law.tpc) {
+    CK(cudaStreamSynchronize(c->st));
+    quiesce(c);
+  }
+  dfree(c->arena, c->law.tlog);
+  dfree(c->arena, c->law.tpc);
   c->law.tlog = nullptr;
   c->law.tpc = nullptr;
-  CK(cudaMalloc(&c->law.tlog, sizeof(float2) * (kLogEntries + 1)));
+  CK(dmalloc(c->arena, &c->law.tlog, sizeof(float2) * (kLogEntries + 1)));
   CK(cudaMemcpy(c->law.tlog, tlog.data(), sizeof(float2) * (kLogEntries + 1), cudaMemcpyHostToDevice));
-  CK(cudaMalloc(&c->law.tpc, sizeof(float4) * (kPcEntries + 1)));
+  CK(dmalloc(c->arena, &c->law.tpc, sizeof(float4) * (kPcEntries + 1)));
   CK(cudaMemcpy(c->law.tpc, tpc.data(), sizeof(float4) * (kPcEntries + 1), cudaMemcpyHostToDevice));
   c->law.hard_cut = hard_cut;
   c->law_n = p.n_mesh;
@@ -213,10 +227,11 @@ static int build_law(tpm_ctx *c) {
 
 // ------------------------------------------------------------------ buffers
 static void free_mesh2(tpm_ctx *c) {
-  if (c->rho2) cudaFree(c->rho2);
-  if (c->spec2) cudaFree(c->spec2);
-  if (c->phi2) cudaFree(c->phi2);
-  if (c->gt) cudaFree(c->gt);
+  quiesce(c);
+  dfree(c->arena, c->rho2);
+  dfree(c->arena, c->spec2);
+  dfree(c->arena, c->phi2);
+  dfree(c->arena, c->gt);
   c->rho2 = nullptr;
   c->spec2 = nullptr;
   c->phi2 = nullptr;
@@ -238,14 +253,14 @@ static int ensure_mesh2(tpm_ctx *c) {
     }
     return 0;
   }
-  CK(cudaMalloc(&c->gt, sizeof(float) * (int64_t)g.n * g.hx * g.n));
+  CK(dmalloc(c->arena, &c->gt, sizeof(float) * (int64_t)g.n * g.hx * g.n));
   launch_green_opt(c->gt, g.n, (double)c->prm.rs_split, c->st);
   CK(cudaGetLastError());
   c->gt_rs = c->prm.rs_split;
   int64_t n3 = (int64_t)g.n * g.n * g.n;
-  CK(cudaMalloc(&c->rho2, sizeof(float) * n3));
-  CK(cudaMalloc(&c->spec2, sizeof(float2) * g.spec_elems));
-  CK(cudaMalloc(&c->phi2, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  CK(dmalloc(c->arena, &c->rho2, sizeof(float) * n3));
+  CK(dmalloc(c->arena, &c->spec2, sizeof(float2) * g.spec_elems));
+  CK(dmalloc(c->arena, &c->phi2, sizeof(float) * (int64_t)g.px * g.py * g.pz));
   CK(cudaMemsetAsync(c->phi2, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz, c->st));
   if (make_phi_tensor_map(g, c->phi2, 4, &c->tmap4b) != 0) return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
   c->gen++;
@@ -254,16 +269,16 @@ static int ensure_mesh2(tpm_ctx *c) {
 
 static void free_mesh(tpm_ctx *c) {
   free_mesh2(c);
-  if (c->pk_acc) cudaFree(c->pk_acc);
+  dfree(c->arena, c->pk_acc);
   c->pk_acc = nullptr;
   c->measure_pk = false;
-  if (c->rho) cudaFree(c->rho);
-  if (c->spec) cudaFree(c->spec);
-  if (c->phi) cudaFree(c->phi);
-  if (c->tile_start) cudaFree(c->tile_start);
-  if (c->cube_start) cudaFree(c->cube_start);
-  if (c->tb.cube_node) cudaFree(c->tb.cube_node);
-  if (c->tb.start_cube) cudaFree(c->tb.start_cube);
+  dfree(c->arena, c->rho);
+  dfree(c->arena, c->spec);
+  dfree(c->arena, c->phi);
+  dfree(c->arena, c->tile_start);
+  dfree(c->arena, c->cube_start);
+  dfree(c->arena, c->tb.cube_node);
+  dfree(c->arena, c->tb.start_cube);
   c->tb.cube_node = c->tb.start_cube = nullptr;
   c->tb.ncubes4 = 0;
   fft_plan_free(c->fp);
@@ -281,18 +296,18 @@ static int alloc_mesh(tpm_ctx *c) {
   c->g = make_geom(c->prm.n_mesh);
   const MeshGeom &g = c->g;
   int64_t n3 = (int64_t)g.n * g.n * g.n;
-  CK(cudaMalloc(&c->rho, sizeof(float) * n3));
-  CK(cudaMalloc(&c->spec, sizeof(float2) * g.spec_elems));
-  CK(cudaMalloc(&c->phi, sizeof(float) * (int64_t)g.px * g.py * g.pz));
+  CK(dmalloc(c->arena, &c->rho, sizeof(float) * n3));
+  CK(dmalloc(c->arena, &c->spec, sizeof(float2) * g.spec_elems));
+  CK(dmalloc(c->arena, &c->phi, sizeof(float) * (int64_t)g.px * g.py * g.pz));
   CK(cudaMemsetAsync(c->phi, 0, sizeof(float) * (int64_t)g.px * g.py * g.pz, c->st));
   uint32_t ntiles = 1u << (3 * (g.cbits - 3));
-  CK(cudaMalloc(&c->tile_start, sizeof(uint32_t) * (ntiles + 1)));
+  CK(dmalloc(c->arena, &c->tile_start, sizeof(uint32_t) * (ntiles + 1)));
   c->ncubes = 1ll << (3 * (g.cbits - 2));
-  CK(cudaMalloc(&c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
+  CK(dmalloc(c->arena, &c->cube_start, sizeof(uint32_t) * (c->ncubes + 1)));
   c->tb.ncubes4 = c->ncubes;
-  CK(cudaMalloc(&c->tb.cube_node, sizeof(uint32_t) * c->ncubes));
-  CK(cudaMalloc(&c->tb.start_cube, sizeof(uint32_t) * (c->ncubes + 1)));
-  fft_plan_init(c->fp, g.n, c->st);
+  CK(dmalloc(c->arena, &c->tb.cube_node, sizeof(uint32_t) * c->ncubes));
+  CK(dmalloc(c->arena, &c->tb.start_cube, sizeof(uint32_t) * (c->ncubes + 1)));
+  CK(fft_plan_init(c->fp, g.n, c->st, c->arena));
   if (make_phi_tensor_map(g, c->phi, 2, &c->tmap2) != 0 || make_phi_tensor_map(g, c->phi, 4, &c->tmap4) != 0)
     return fail(TPM_E_CUDA, "cuTensorMapEncodeTiled failed");
   CK(cudaGetLastError());
@@ -305,8 +320,9 @@ static void free_particles(tpm_ctx *c) {
   void *ps[] = {c->pos, c->vel, c->key, c->key_alt, c->val, c->val_alt, c->spos, c->fpm, c->ftree, c->fout,
                 c->ss.hist, c->ss.dtotal, c->tb.start, c->tb.count, c->tb.child, c->tb.nchild, c->tb.level, c->tb.geo,
                 c->tb.mom0, c->tb.mom1, c->tb.mom2, c->tb.walkA, c->tb.walkB, c->tb.tile_sum, c->tb.groups};
+  quiesce(c);
   for (void *p : ps)
-    if (p) cudaFree(p);
+    dfree(c->arena, p);
   c->pos = nullptr;
   c->vel = nullptr;
   c->key = c->key_alt = nullptr;
@@ -331,43 +347,43 @@ static int ensure_particles(tpm_ctx *c, int64_t np) {
   free_particles(c);
   c->gen++;
   int64_t cap = np;
-  CK(cudaMalloc(&c->pos, sizeof(uint32_t) * 3 * cap));
-  CK(cudaMalloc(&c->vel, sizeof(float) * 3 * cap));
-  CK(cudaMalloc(&c->key, sizeof(uint64_t) * cap));
-  CK(cudaMalloc(&c->key_alt, sizeof(uint64_t) * cap));
-  CK(cudaMalloc(&c->val, sizeof(uint32_t) * cap));
-  CK(cudaMalloc(&c->val_alt, sizeof(uint32_t) * cap));
-  CK(cudaMalloc(&c->spos, sizeof(uint32_t) * 3 * cap));
-  CK(cudaMalloc(&c->fpm, sizeof(float) * 3 * cap));
-  CK(cudaMalloc(&c->ftree, sizeof(float) * 3 * cap));
-  CK(cudaMalloc(&c->fout, sizeof(float) * 3 * cap));
+  CK(dmalloc(c->arena, &c->pos, sizeof(uint32_t) * 3 * cap));
+  CK(dmalloc(c->arena, &c->vel, sizeof(float) * 3 * cap));
+  CK(dmalloc(c->arena, &c->key, sizeof(uint64_t) * cap));
+  CK(dmalloc(c->arena, &c->key_alt, sizeof(uint64_t) * cap));
+  CK(dmalloc(c->arena, &c->val, sizeof(uint32_t) * cap));
+  CK(dmalloc(c->arena, &c->val_alt, sizeof(uint32_t) * cap));
+  CK(dmalloc(c->arena, &c->spos, sizeof(uint32_t) * 3 * cap));
+  CK(dmalloc(c->arena, &c->fpm, sizeof(float) * 3 * cap));
+  CK(dmalloc(c->arena, &c->ftree, sizeof(float) * 3 * cap));
+  CK(dmalloc(c->arena, &c->fout, sizeof(float) * 3 * cap));
   int64_t ntiles = sort_tiles(cap);
-  CK(cudaMalloc(&c->ss.hist, sizeof(uint32_t) * 256 * (ntiles + 1)));
-  CK(cudaMalloc(&c->ss.dtotal, sizeof(uint32_t) * 256));
+  CK(dmalloc(c->arena, &c->ss.hist, sizeof(uint32_t) * 256 * (ntiles + 1)));
+  CK(dmalloc(c->arena, &c->ss.dtotal, sizeof(uint32_t) * 256));
   c->ss.cap_tiles = ntiles;
   // tree: every node holds >= 1 particle and every inner node >= 10, so the
   // node count is bounded by the leaves (<= np) plus the inner nodes
   int64_t cap_nodes = cap + cap / 4 + 64;
   TreeBuffers &tb = c->tb;
   tb.cap_nodes = cap_nodes;
-  CK(cudaMalloc(&tb.start, sizeof(uint32_t) * cap_nodes));
-  CK(cudaMalloc(&tb.count, sizeof(uint32_t) * cap_nodes));
-  CK(cudaMalloc(&tb.child, sizeof(uint32_t) * cap_nodes));
-  CK(cudaMalloc(&tb.nchild, sizeof(uint32_t) * cap_nodes));
-  CK(cudaMalloc(&tb.level, sizeof(uint8_t) * cap_nodes));
-  CK(cudaMalloc(&tb.geo, sizeof(uint4) * cap_nodes));
-  CK(cudaMalloc(&tb.mom0, sizeof(float4) * cap_nodes));
-  CK(cudaMalloc(&tb.mom1, sizeof(float4) * cap_nodes));
-  CK(cudaMalloc(&tb.mom2, sizeof(float4) * cap_nodes));
-  CK(cudaMalloc(&tb.walkA, sizeof(uint4) * 2 * cap_nodes));
-  CK(cudaMalloc(&tb.walkB, sizeof(uint4) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.start, sizeof(uint32_t) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.count, sizeof(uint32_t) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.child, sizeof(uint32_t) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.nchild, sizeof(uint32_t) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.level, sizeof(uint8_t) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.geo, sizeof(uint4) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.mom0, sizeof(float4) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.mom1, sizeof(float4) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.mom2, sizeof(float4) * cap_nodes));
+  CK(dmalloc(c->arena, &tb.walkA, sizeof(uint4) * 2 * cap_nodes));
+  CK(dmalloc(c->arena, &tb.walkB, sizeof(uint4) * cap_nodes));
   int64_t ts = (cap_nodes + 1023) / 1024 + 16;
   int64_t need_groups = 2 * c->ncubes + (c->ncubes + 4095) / 4096 + 16;
   if (ts < need_groups) ts = need_groups;
   tb.cap_tiles = ts;
-  CK(cudaMalloc(&tb.tile_sum, sizeof(uint32_t) * ts));
+  CK(dmalloc(c->arena, &tb.tile_sum, sizeof(uint32_t) * ts));
   tb.cap_groups = cap / 1 + c->ncubes + 16;
-  CK(cudaMalloc(&tb.groups, sizeof(uint32_t) * 2 * tb.cap_groups));
+  CK(dmalloc(c->arena, &tb.groups, sizeof(uint32_t) * 2 * tb.cap_groups));
   c->cap = cap;
   return 0;
 }
@@ -554,6 +570,12 @@ int tpm_device_count(void) {
 }
 
 int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
+  return tpm::create_ctx(params, device, nullptr, out);
+}
+
+}  // extern "C"
+
+int tpm::create_ctx(const tpm_params *params, int device, DeviceArena *arena, tpm_ctx **out) {
   if (!out) return fail(TPM_E_ARG, "out is NULL");
   *out = nullptr;
   int rc = check_params(params);
@@ -568,6 +590,7 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
   tpm_ctx *c = new tpm_ctx();
   c->prm = *params;
   c->device = device;
+  c->arena = arena;
   memset(c->stage_ms, 0, sizeof(c->stage_ms));
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
@@ -583,21 +606,21 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
     }
   }
   // the allocations below are mirrored by ctx_bytes()
-  if (cudaMalloc(&c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
-      cudaMalloc(&c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
-      cudaMalloc(&c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess ||
-      cudaMalloc(&c->tb.walkbox, sizeof(WalkBox)) != cudaSuccess) {
+  if (dmalloc(c->arena, &c->err, sizeof(uint32_t) * 8) != cudaSuccess ||
+      dmalloc(c->arena, &c->tb.counters, sizeof(uint32_t) * 16) != cudaSuccess ||
+      dmalloc(c->arena, &c->tb.level_range, sizeof(uint32_t) * 2 * (kAxisBits + 2)) != cudaSuccess ||
+      dmalloc(c->arena, &c->tb.walkbox, sizeof(WalkBox)) != cudaSuccess) {
     tpm_destroy(c);
     return fail(TPM_E_NOMEM, "cudaMalloc of context scratch failed");
   }
   c->tb.stack_words = walk_stack_words();
-  if (cudaMalloc(&c->tb.stack, sizeof(uint32_t) * c->tb.stack_words) != cudaSuccess) {
+  if (dmalloc(c->arena, &c->tb.stack, sizeof(uint32_t) * c->tb.stack_words) != cudaSuccess) {
     tpm_destroy(c);
     return fail(TPM_E_NOMEM, "cudaMalloc of walk stacks failed");
   }
   if (cudaMallocHost(&c->herr, sizeof(uint32_t) * 8) != cudaSuccess ||
       cudaMallocHost(&c->hfac, sizeof(double) * kFacWords) != cudaSuccess ||
-      cudaMalloc(&c->dfac, sizeof(double) * kFacWords) != cudaSuccess) {
+      dmalloc(c->arena, &c->dfac, sizeof(double) * kFacWords) != cudaSuccess) {
     tpm_destroy(c);
     return fail(TPM_E_NOMEM, "allocation of step scratch failed");
   }
@@ -616,28 +639,31 @@ int tpm_create(const tpm_params *params, int device, tpm_ctx **out) {
   return 0;
 }
 
+extern "C" {
+
 int tpm_destroy(tpm_ctx *c) {
   if (!c) return 0;
   cudaSetDevice(c->device);
   if (c->st) cudaStreamSynchronize(c->st);
+  quiesce(c);
   free_stream_state(c);
   free_particles(c);
   free_mesh(c);
-  if (c->law.tlog) cudaFree(c->law.tlog);
-  if (c->law.tpc) cudaFree(c->law.tpc);
-  if (c->err) cudaFree(c->err);
-  if (c->tb.counters) cudaFree(c->tb.counters);
-  if (c->tb.level_range) cudaFree(c->tb.level_range);
-  if (c->tb.walkbox) cudaFree(c->tb.walkbox);
-  if (c->tb.stack) cudaFree(c->tb.stack);
-  if (c->stage) cudaFree(c->stage);
+  dfree(c->arena, c->law.tlog);
+  dfree(c->arena, c->law.tpc);
+  dfree(c->arena, c->err);
+  dfree(c->arena, c->tb.counters);
+  dfree(c->arena, c->tb.level_range);
+  dfree(c->arena, c->tb.walkbox);
+  dfree(c->arena, c->tb.stack);
+  dfree(c->arena, c->stage);
   for (CapturedGraph &gr : c->graphs) {
     if (gr.exec) cudaGraphExecDestroy(gr.exec);
     if (gr.graph) cudaGraphDestroy(gr.graph);
   }
   if (c->herr) cudaFreeHost(c->herr);
   if (c->hfac) cudaFreeHost(c->hfac);
-  if (c->dfac) cudaFree(c->dfac);
+  dfree(c->arena, c->dfac);
   for (int i = 0; i <= kNStages; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -698,10 +724,11 @@ int tpm_load_fixed(tpm_ctx *c, int64_t np, const uint32_t *pos, const float *vel
 
 static int ensure_stage(tpm_ctx *c, size_t bytes) {
   if (bytes <= c->stage_bytes) return 0;
-  if (c->stage) cudaFree(c->stage);
+  if (c->stage) quiesce(c);
+  dfree(c->arena, c->stage);
   c->stage = nullptr;
   c->stage_bytes = 0;
-  CK(cudaMalloc(&c->stage, bytes));
+  CK(dmalloc(c->arena, &c->stage, bytes));
   c->stage_bytes = bytes;
   return 0;
 }

@@ -60,14 +60,35 @@ MeshGeom make_geom(int n);
 // moved by half a cell along every axis (a second launch).
 void launch_tsc_deposit(const MeshGeom &g, const uint32_t *spos, const uint32_t *tile_start,
                         float mass, float *rho, cudaStream_t st, float *rho2 = nullptr);
+// Device memory arena (arena.cu): large blocks claimed from the driver once,
+// sub-ranges handed out best fit and merged back on release. Thread-safe.
+struct DeviceArena;
+// step_bytes: the size of each block claimed when nothing free fits (<= 0: 1 GiB)
+DeviceArena *arena_create(int device, int64_t step_bytes);
+// frees every block; no range may be in use
+void arena_destroy(DeviceArena *a);
+// claims a block so that at least `bytes` are free
+cudaError_t arena_reserve(DeviceArena *a, int64_t bytes);
+void arena_usage(DeviceArena *a, int64_t *reserved, int64_t *in_use);
+cudaError_t arena_alloc(DeviceArena *a, void **p, size_t bytes);
+void arena_free(DeviceArena *a, void *p);
+// From the arena when a is given, else cudaMalloc / cudaFree.
+cudaError_t dmalloc(DeviceArena *a, void **p, size_t bytes);
+void dfree(DeviceArena *a, void *p);
+template <class T>
+cudaError_t dmalloc(DeviceArena *a, T **p, size_t bytes) {
+  return dmalloc(a, reinterpret_cast<void **>(p), bytes);
+}
+
 // FFT pipeline: rho (n^3 real) -> phi_pad (ghosted potential).
 struct FftPlan {
   float2 *tw = nullptr;   // twiddles exp(-2 pi i k / L) for L = n and L = n/2
   float2 *tw_half = nullptr;
   int n = 0;
+  DeviceArena *arena = nullptr;  // where the twiddles live (nullptr: cudaMalloc)
 };
 // twiddle tables are written on st
-void fft_plan_init(FftPlan &p, int n, cudaStream_t st);
+cudaError_t fft_plan_init(FftPlan &p, int n, cudaStream_t st, DeviceArena *arena = nullptr);
 // plain unnormalised transforms: real [z][y][x] -> spec [z][y][hx] (e^{-i}),
 // spec -> ghosted real (e^{+i}; spec is overwritten)
 void fft_forward(const MeshGeom &g, const FftPlan &p, const float *real, float2 *spec, cudaStream_t st);

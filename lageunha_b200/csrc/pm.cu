@@ -564,22 +564,25 @@ __global__ void k_fft_cols(float2 *__restrict__ spec, float2 *__restrict__ spec2
                            const float2 *__restrict__ tw_n, int axis, float dir, int with_green, struct GreenArgs ga,
                            int TX, int nspec);
 
-void fft_plan_init(FftPlan &p, int n, cudaStream_t st) {
+cudaError_t fft_plan_init(FftPlan &p, int n, cudaStream_t st, DeviceArena *arena) {
   p.n = n;
+  p.arena = arena;
   const int max_smem = 160 * 1024;
   cudaFuncSetAttribute(k_fft_x_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   cudaFuncSetAttribute(k_fft_x_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-  cudaMalloc(&p.tw, sizeof(float2) * n);
-  k_twiddles<<<(n + 255) / 256, 256, 0, st>>>(p.tw, n);
   int h = n / 2 > 0 ? n / 2 : 1;
-  cudaMalloc(&p.tw_half, sizeof(float2) * h);
+  cudaError_t e = dmalloc(arena, &p.tw, sizeof(float2) * n);
+  if (e == cudaSuccess) e = dmalloc(arena, &p.tw_half, sizeof(float2) * h);
+  if (e != cudaSuccess) return e;
+  k_twiddles<<<(n + 255) / 256, 256, 0, st>>>(p.tw, n);
   k_twiddles<<<(h + 255) / 256, 256, 0, st>>>(p.tw_half, h);
+  return cudaGetLastError();
 }
 
 void fft_plan_free(FftPlan &p) {
-  if (p.tw) cudaFree(p.tw);
-  if (p.tw_half) cudaFree(p.tw_half);
+  dfree(p.arena, p.tw);
+  dfree(p.arena, p.tw_half);
   p.tw = p.tw_half = nullptr;
 }
 

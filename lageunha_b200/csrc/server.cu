@@ -1,21 +1,28 @@
 // The request loop: continuous batching of force and step requests for boxes
 // of different sizes on one GPU.
 //
-// Clients submit requests (tpm_server_submit) from any thread; one worker
-// thread owns every CUDA call. Each loop of the worker
-//   * admits queued requests in arrival order while their device footprint
-//     (tpm_estimate_bytes) fits under the HBM cap and in the device's free
-//     memory, skipping over requests that do not fit yet so that small boxes
-//     are not held behind a large one;
-//   * gives each admitted request a context, reused from a pool of idle
-//     contexts of the same mesh size when one exists, and uploads its
-//     particles (pinned staging when the caller's buffers are pageable);
-//   * launches the next step (a captured step graph, or the captured force
-//     graph for a force request) of every active request whose previous
-//     launch has finished: requests progress independently, so work from
-//     requests admitted at different times overlaps on the device;
-//   * retires finished requests: results to the caller's buffers, context
+// Clients submit requests (tpm_server_submit) from any thread. Two threads
+// serve them:
+//   * the admission thread takes queued requests in arrival order while their
+//     device footprint (tpm_estimate_bytes) fits under the HBM cap and in the
+//     device's free memory, skipping over requests that do not fit yet so
+//     that small boxes are not held behind a large one. It gives each
+//     admitted request a context, reused from a pool of idle contexts of the
+//     same mesh size when one exists, uploads its particles (pinned staging
+//     when the caller's buffers are pageable) and captures its graph, then
+//     hands it to the launch thread. Creating a context, its first upload and
+//     its capture take 10-60 ms; the launch thread keeps stepping the active
+//     requests meanwhile.
+//   * the launch thread launches the next step (a captured step graph, or the
+//     captured force graph for a force request) of every active request whose
+//     previous launch has finished: requests progress independently, so work
+//     from requests admitted at different times overlaps on the device. It
+//     retires finished requests: results to the caller's buffers, context
 //     back to the pool, timestamps recorded.
+// The two threads share the pool, the byte accounting and the hand-over list
+// under the server's mutex, held for bookkeeping only, never across a CUDA
+// call. Each context belongs to one thread at a time. Graph capture runs in
+// the relaxed mode, so the launch thread's calls are legal during a capture.
 // Device state (particles, mesh, tree, graphs) stays resident between the
 // steps of a request. A request's result does not depend on what else is in
 // flight: each context has its own buffers, stream and graphs.
@@ -38,9 +45,16 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+constexpr int kNStats = 12;
+
+int64_t usec_since(Clock::time_point t) {
+  return std::chrono::duration_cast<std::chrono::microseconds>(Clock::now() - t).count();
+}
+
 enum Phase { kQueued = 0, kRunning, kDraining, kDone, kFailed };
 
 struct Req {
+  tpm_server *srv = nullptr;
   int64_t id = 0;
   tpm_request r;
   int phase = kQueued;
@@ -82,28 +96,44 @@ struct tpm_server {
   int64_t cap = 0;
   int max_active = 0;
   Clock::time_point t0;
-  std::thread worker;
+  // the contexts' device buffers: claimed from the driver in large blocks,
+  // kept across requests
+  DeviceArena *arena = nullptr;
+  std::thread admitter, launcher;
+  // guards every field below except queue and active
   std::mutex mu;
-  std::condition_variable cv_submit, cv_done;
+  std::condition_variable cv_submit;  // wakes the admission thread: a request arrived or one retired
+  std::condition_variable cv_ready;   // wakes the launch thread: a request was admitted
+  std::condition_variable cv_done;    // wakes clients in tpm_server_wait
   bool stop = false;
+  bool admit_done = false;                // the admission thread has left
   int64_t next_id = 1;
-  std::deque<Req *> incoming;             // submitted, not yet seen by the worker
+  std::deque<Req *> incoming;             // submitted, not yet seen by the admission thread
   std::map<int64_t, Req *> all;           // every request by id
-  // worker-only state
-  std::vector<Req *> queue;               // waiting for admission, arrival order
-  std::vector<Req *> active;
+  std::vector<Req *> ready;               // admitted, not yet taken by the launch thread
+  int completions = 0;                    // launches seen finished by the stream callbacks
   std::vector<PoolEntry> pool;            // idle contexts
   int64_t bytes_active = 0, bytes_pool = 0;
-  int64_t stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int live = 0;                           // requests ready or active
+  int64_t stats[kNStats] = {};
   // [0] done [1] failed [2] peak active [3] peak bytes [4] contexts created
   // [5] contexts reused [6] contexts evicted [7] admissions deferred for memory
+  // admission thread time, microseconds: [8] making or re-parameterising
+  // contexts [9] uploading particles [10] capturing graphs [11] reserving
+  // memory (evictions included); tpm_server_stats adds [12] the arena's bytes
+  // admission-thread only
+  std::vector<Req *> queue;               // waiting for admission, arrival order
+  // launch-thread only
+  std::vector<Req *> active;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
 
 namespace {
 
-void finish(tpm_server *s, Req *q, int status, const char *msg) {
+// Records q's outcome. A request that was handed to the launch thread
+// (retiring) frees its slot and wakes the admission thread.
+void finish(tpm_server *s, Req *q, int status, const char *msg, bool retiring) {
   std::lock_guard<std::mutex> lk(s->mu);
   q->status = status;
   if (status) {
@@ -115,13 +145,23 @@ void finish(tpm_server *s, Req *q, int status, const char *msg) {
     s->stats[0]++;
   }
   q->t_done = s->now();
+  if (retiring) {
+    s->live--;
+    s->cv_submit.notify_one();
+  }
   s->cv_done.notify_all();
 }
 
-void release_ctx(tpm_server *s, Req *q) {
+// q's context back to the pool (a device error destroys it instead), its
+// event and staging freed.
+void release_ctx(tpm_server *s, Req *q, bool broken) {
   if (q->ctx) {
-    s->pool.push_back(PoolEntry{q->ctx, q->bytes, s->now()});
-    s->bytes_pool += q->bytes;
+    if (broken) tpm_destroy(q->ctx);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!broken) {
+      s->pool.push_back(PoolEntry{q->ctx, q->bytes, s->now()});
+      s->bytes_pool += q->bytes;
+    }
     s->bytes_active -= q->bytes;
     q->ctx = nullptr;
   }
@@ -131,38 +171,74 @@ void release_ctx(tpm_server *s, Req *q) {
   q->stage = nullptr;
 }
 
-void evict_one(tpm_server *s) {
-  // the least recently used idle context
+// Takes the least recently used idle context out of the pool; the caller
+// holds s->mu and destroys the context after releasing it.
+tpm_ctx *take_lru(tpm_server *s) {
   auto it = std::min_element(s->pool.begin(), s->pool.end(),
                              [](const PoolEntry &a, const PoolEntry &b) { return a.last_used < b.last_used; });
-  if (it == s->pool.end()) return;
-  tpm_destroy(it->ctx);
+  if (it == s->pool.end()) return nullptr;
+  tpm_ctx *c = it->ctx;
   s->bytes_pool -= it->bytes;
   s->pool.erase(it);
   s->stats[6]++;
+  return c;
 }
 
-// A context for q from the pool (same mesh size, enough capacity) or new.
-int acquire_ctx(tpm_server *s, Req *q) {
+// Reserves q's device bytes: an idle context of the same mesh size and
+// enough capacity (no new memory), else room under the cap, evicting idle
+// contexts least recently used first. False when q does not fit yet.
+bool reserve(tpm_server *s, Req *q) {
   const tpm_request &r = q->r;
-  for (size_t i = 0; i < s->pool.size(); i++) {
-    PoolEntry &p = s->pool[i];
-    if (p.ctx->prm.n_mesh == r.params.n_mesh && p.ctx->cap >= r.np) {
-      q->ctx = p.ctx;
-      q->bytes = p.bytes;
-      s->bytes_pool -= p.bytes;
-      s->pool.erase(s->pool.begin() + i);
-      s->stats[5]++;
-      return tpm_set_params(q->ctx, &r.params);
+  const int64_t need = ctx_bytes(r.params.n_mesh, r.np);
+  std::vector<tpm_ctx *> evicted;
+  bool fits = true;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (size_t i = 0; i < s->pool.size(); i++) {
+      PoolEntry &p = s->pool[i];
+      if (p.ctx->prm.n_mesh == r.params.n_mesh && p.ctx->cap >= r.np) {
+        q->ctx = p.ctx;
+        q->bytes = p.bytes;
+        s->bytes_pool -= p.bytes;
+        s->bytes_active += p.bytes;
+        s->pool.erase(s->pool.begin() + i);
+        s->stats[5]++;
+        return true;
+      }
+    }
+    while (s->bytes_active + s->bytes_pool + need > s->cap && !s->pool.empty()) evicted.push_back(take_lru(s));
+    if (s->bytes_active + s->bytes_pool + need > s->cap) {
+      fits = false;
+    } else {
+      q->bytes = need;
+      s->bytes_active += need;
     }
   }
-  tpm_ctx *c = nullptr;
-  int rc = tpm_create(&r.params, s->device, &c);
-  if (rc) return rc;
-  q->ctx = c;
-  q->bytes = ctx_bytes(r.params.n_mesh, r.np);
-  s->stats[4]++;
-  return 0;
+  for (tpm_ctx *c : evicted) tpm_destroy(c);
+  if (!fits) return false;
+  // the device's free memory too (other processes share the GPU), beside
+  // what the arena holds unused
+  const int64_t margin = 512ll << 20;
+  size_t fr = 0, tot = 0;
+  auto available = [&]() {
+    int64_t reserved = 0, in_use = 0;
+    arena_usage(s->arena, &reserved, &in_use);
+    return (int64_t)fr + (reserved - in_use);
+  };
+  while (cudaMemGetInfo(&fr, &tot) == cudaSuccess && available() < need + margin) {
+    tpm_ctx *c = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      c = take_lru(s);
+      if (!c) {
+        s->bytes_active -= need;
+        q->bytes = 0;
+        return false;
+      }
+    }
+    tpm_destroy(c);
+  }
+  return true;
 }
 
 // Uploads the particles and prepares the per-request event and staging.
@@ -190,10 +266,26 @@ int start(tpm_server *s, Req *q) {
       vel = (const float *)((char *)q->stage + nb);
     }
   }
+  Clock::time_point t = Clock::now();
   int rc = tpm_load_fixed(c, r.np, pos, vel, TPM_MEM_HOST);
   if (rc) return rc;
-  if (r.nsteps == 0) return ensure_graph(c, kGraphAll);
-  return ensure_graph(c, kGraphStep);
+  int64_t t_load = usec_since(t);
+  t = Clock::now();
+  rc = ensure_graph(c, r.nsteps == 0 ? kGraphAll : kGraphStep);
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->stats[9] += t_load;
+  s->stats[10] += usec_since(t);
+  return rc;
+}
+
+// Runs on the CUDA callback thread when a launch of q has finished: wakes
+// the launch thread. Every context's stream is synchronized before the
+// context is destroyed, so no callback outlives the server.
+void CUDART_CB on_launch_done(void *p) {
+  tpm_server *s = static_cast<Req *>(p)->srv;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->completions++;
+  s->cv_ready.notify_one();
 }
 
 // Launches the next unit of work of q (one step, or the force evaluation).
@@ -219,6 +311,7 @@ int launch_next(tpm_server *s, Req *q) {
     CK(cudaGraphLaunch(c->graphs[kGraphStep].exec, c->st));
   }
   CK(cudaEventRecord(q->ev, c->st));
+  CK(cudaLaunchHostFunc(c->st, on_launch_done, q));
   q->step++;
   q->inflight = true;
   return 0;
@@ -245,6 +338,7 @@ int drain(tpm_server *s, Req *q) {
     CK(cudaMemcpyAsync(dst, c->vel, nb, cudaMemcpyDeviceToHost, c->st));
   }
   CK(cudaEventRecord(q->ev, c->st));
+  CK(cudaLaunchHostFunc(c->st, on_launch_done, q));
   q->inflight = true;
   return 0;
 }
@@ -257,83 +351,125 @@ void copy_out_staged(Req *q) {
   if (r.force_out && !q->out_pinned[2]) memcpy(r.force_out, (char *)q->stage + 2 * nb, nb);
 }
 
+// Admits q: reserve its bytes, take or create its context, upload, capture,
+// hand it to the launch thread. False when q does not fit yet; true when q
+// was consumed, admitted or failed.
 bool try_admit(tpm_server *s, Req *q) {
-  int64_t need = ctx_bytes(q->r.params.n_mesh, q->r.np);
-  // an idle context of this mesh with the capacity is reused without new memory
-  bool reusable = false;
-  for (const PoolEntry &p : s->pool)
-    if (p.ctx->prm.n_mesh == q->r.params.n_mesh && p.ctx->cap >= q->r.np) reusable = true;
-  if (!reusable) {
-    while (s->bytes_active + s->bytes_pool + need > s->cap && !s->pool.empty()) evict_one(s);
-    if (s->bytes_active + s->bytes_pool + need > s->cap) return false;
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
-      const int64_t margin = 512ll << 20;
-      while ((int64_t)fr < need + margin && !s->pool.empty()) {
-        evict_one(s);
-        cudaMemGetInfo(&fr, &tot);
-      }
-      if ((int64_t)fr < need + margin) return false;
-    }
+  Clock::time_point t = Clock::now();
+  bool fits = reserve(s, q);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats[11] += usec_since(t);
   }
-  int rc = acquire_ctx(s, q);
-  if (!rc) {
-    s->bytes_active += q->bytes;
-    q->t_admit = s->now();
-    rc = start(s, q);
-  }
-  if (rc) {
-    std::string m = last_error_string();
-    if (q->ctx) {
-      tpm_destroy(q->ctx);
-      s->bytes_active -= q->bytes;
-      q->ctx = nullptr;
-    }
-    if (q->ev) cudaEventDestroy(q->ev);
-    q->ev = nullptr;
-    if (q->stage) cudaFreeHost(q->stage);
-    q->stage = nullptr;
-    finish(s, q, rc, m.c_str());
-    return true;  // consumed (failed)
+  if (!fits) return false;
+  t = Clock::now();
+  int rc = 0;
+  bool created = false;
+  if (q->ctx) {
+    rc = tpm_set_params(q->ctx, &q->r.params);
+  } else {
+    rc = create_ctx(&q->r.params, s->device, s->arena, &q->ctx);
+    created = !rc;
   }
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    q->phase = kRunning;
+    if (created) s->stats[4]++;
+    s->stats[8] += usec_since(t);
+    q->t_admit = s->now();
   }
-  s->active.push_back(q);
-  s->stats[2] = std::max<int64_t>(s->stats[2], (int64_t)s->active.size());
+  if (!rc) rc = start(s, q);
+  if (rc) {
+    std::string m = last_error_string();
+    if (!q->ctx) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->bytes_active -= q->bytes;
+    }
+    release_ctx(s, q, true);
+    q->bytes = 0;
+    if (rc == TPM_E_NOMEM) {
+      // out of device memory (the free ranges too fragmented, or another
+      // process took the memory): the idle contexts go back to the arena and
+      // q waits for a retry, unless nothing else holds memory
+      std::vector<tpm_ctx *> idle;
+      bool others;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        while (tpm_ctx *c = take_lru(s)) idle.push_back(c);
+        others = s->live > 0 || !idle.empty();
+      }
+      for (tpm_ctx *c : idle) tpm_destroy(c);
+      if (others) return false;
+    }
+    finish(s, q, rc, m.c_str(), false);
+    return true;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  q->phase = kRunning;
+  s->ready.push_back(q);
+  s->live++;
+  s->stats[2] = std::max<int64_t>(s->stats[2], (int64_t)s->live);
   s->stats[3] = std::max<int64_t>(s->stats[3], s->bytes_active + s->bytes_pool);
+  s->cv_ready.notify_one();
   return true;
 }
 
-void worker_main(tpm_server *s) {
+void admit_main(tpm_server *s) {
   cudaSetDevice(s->device);
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      if (s->incoming.empty() && s->queue.empty() && s->active.empty()) {
-        if (s->stop) break;
-        s->cv_submit.wait_for(lk, std::chrono::milliseconds(5));
-      }
       while (!s->incoming.empty()) {
         s->queue.push_back(s->incoming.front());
         s->incoming.pop_front();
       }
+      if (s->queue.empty()) {
+        if (s->stop) break;
+        s->cv_submit.wait_for(lk, std::chrono::milliseconds(5));
+        continue;
+      }
     }
-    bool progressed = false;
-    // admission, arrival order, skipping what does not fit yet
+    // arrival order, skipping what does not fit yet
+    bool admitted = false;
     for (size_t i = 0; i < s->queue.size();) {
-      if ((int)s->active.size() >= s->max_active) break;
-      Req *q = s->queue[i];
-      if (try_admit(s, q)) {
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->live >= s->max_active) break;
+      }
+      if (try_admit(s, s->queue[i])) {
         s->queue.erase(s->queue.begin() + i);
-        progressed = true;
+        admitted = true;
       } else {
+        std::lock_guard<std::mutex> lk(s->mu);
         s->stats[7]++;
         i++;
       }
     }
-    // launches and completions
+    if (!admitted) {
+      // until a request retires (a slot or memory freed) or arrives
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->incoming.empty()) s->cv_submit.wait_for(lk, std::chrono::milliseconds(2));
+    }
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->admit_done = true;
+  s->cv_ready.notify_all();
+}
+
+void launch_main(tpm_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    {
+      // sleep until a request is admitted or a launch finishes; the timeout
+      // only bounds the wait should a callback never come
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->ready.empty() && s->completions == 0) {
+        if (s->active.empty() && s->admit_done) break;
+        s->cv_ready.wait_for(lk, std::chrono::milliseconds(2));
+      }
+      s->completions = 0;
+      for (Req *q : s->ready) s->active.push_back(q);
+      s->ready.clear();
+    }
     for (size_t i = 0; i < s->active.size();) {
       Req *q = s->active[i];
       int rc = 0;
@@ -345,13 +481,12 @@ void worker_main(tpm_server *s) {
           continue;
         }
         q->inflight = false;
-        progressed = true;
         if (e != cudaSuccess) {
           rc = fail(TPM_E_CUDA, "request %lld: %s", (long long)q->id, cudaGetErrorString(e));
         } else if (q->phase == kDraining) {
           copy_out_staged(q);
-          release_ctx(s, q);
-          finish(s, q, 0, nullptr);
+          release_ctx(s, q, false);
+          finish(s, q, 0, nullptr, true);
           retired = true;
         } else {
           rc = finish_forces(q->ctx, TPM_PART_ALL, true, false);
@@ -369,19 +504,13 @@ void worker_main(tpm_server *s) {
           }
           rc = drain(s, q);
         }
-        progressed = true;
       }
       if (rc) {
         std::string m = last_error_string();
         if (q->ctx) cudaStreamSynchronize(q->ctx->st);
         // a context that saw a device error is not reused
-        if (q->ctx) {
-          tpm_destroy(q->ctx);
-          s->bytes_active -= q->bytes;
-          q->ctx = nullptr;
-        }
-        release_ctx(s, q);
-        finish(s, q, rc, m.c_str());
+        release_ctx(s, q, true);
+        finish(s, q, rc, m.c_str(), true);
         retired = true;
       }
       if (retired) {
@@ -390,10 +519,14 @@ void worker_main(tpm_server *s) {
         i++;
       }
     }
-    if (!progressed && !s->active.empty()) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
-  for (PoolEntry &p : s->pool) tpm_destroy(p.ctx);
-  s->pool.clear();
+  std::vector<PoolEntry> idle;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    idle.swap(s->pool);
+    s->bytes_pool = 0;
+  }
+  for (PoolEntry &p : idle) tpm_destroy(p.ctx);
 }
 
 }  // namespace
@@ -414,7 +547,9 @@ int tpm_server_create(int device, int64_t hbm_cap_bytes, int32_t max_active, tpm
   s->cap = hbm_cap_bytes;
   s->max_active = max_active;
   s->t0 = Clock::now();
-  s->worker = std::thread(worker_main, s);
+  s->arena = arena_create(device, 0);
+  s->admitter = std::thread(admit_main, s);
+  s->launcher = std::thread(launch_main, s);
   *out = s;
   return 0;
 }
@@ -430,6 +565,7 @@ int tpm_server_submit(tpm_server *s, const tpm_request *req, int64_t *id) {
     return fail(TPM_E_NOMEM, "request needs %lld bytes, above the server's cap",
                 (long long)ctx_bytes(req->params.n_mesh, req->np));
   Req *q = new Req();
+  q->srv = s;
   q->r = *req;
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) {
@@ -491,9 +627,20 @@ int tpm_server_wait(tpm_server *s, int64_t id, double timeout_s) {
 int tpm_server_stats(tpm_server *s, int64_t *out, int n) {
   if (!s || !out) return fail(TPM_E_ARG, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
-  int k = n < 8 ? n : 8;
-  for (int i = 0; i < k; i++) out[i] = s->stats[i];
+  int64_t all[kNStats + 1];
+  for (int i = 0; i < kNStats; i++) all[i] = s->stats[i];
+  arena_usage(s->arena, &all[kNStats], nullptr);
+  int k = n < kNStats + 1 ? n : kNStats + 1;
+  for (int i = 0; i < k; i++) out[i] = all[i];
   return k;
+}
+
+int tpm_server_reserve(tpm_server *s, int64_t bytes) {
+  if (!s || bytes < 0) return fail(TPM_E_ARG, "bad arguments to tpm_server_reserve");
+  if (bytes > s->cap) return fail(TPM_E_ARG, "reserve of %lld bytes above the server's cap", (long long)bytes);
+  CK(cudaSetDevice(s->device));
+  CK(arena_reserve(s->arena, bytes));
+  return 0;
 }
 
 int tpm_server_destroy(tpm_server *s) {
@@ -503,7 +650,10 @@ int tpm_server_destroy(tpm_server *s) {
     s->stop = true;
     s->cv_submit.notify_all();
   }
-  if (s->worker.joinable()) s->worker.join();
+  if (s->admitter.joinable()) s->admitter.join();
+  if (s->launcher.joinable()) s->launcher.join();
+  // every context is destroyed by now: the arena's blocks go back to the driver
+  arena_destroy(s->arena);
   for (auto &kv : s->all) delete kv.second;
   delete s;
   return 0;

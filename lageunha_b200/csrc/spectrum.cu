@@ -21,7 +21,7 @@ extern "C" {
 int tpm_set_power_spectrum(tpm_ctx *c, int enable) {
   if (!c) return fail(TPM_E_ARG, "ctx is NULL");
   CK(cudaSetDevice(c->device));
-  if (enable && !c->pk_acc) CK(cudaMalloc(&c->pk_acc, sizeof(double) * 2 * (c->g.n + 1)));
+  if (enable && !c->pk_acc) CK(dmalloc(c->arena, &c->pk_acc, sizeof(double) * 2 * (c->g.n + 1)));
   bool want = enable != 0;
   if (want != c->measure_pk) c->gen++;
   c->measure_pk = want;

@@ -37,15 +37,15 @@ int ensure_slots(tpm_ctx *c, int64_t np) {
   CK(cudaStreamSynchronize(c->st));
   CK(cudaStreamSynchronize(sp.out));
   for (int s = 0; s < 2; s++) {
-    if (sp.pos[s]) cudaFree(sp.pos[s]);
-    if (sp.force[s]) cudaFree(sp.force[s]);
+    dfree(c->arena, sp.pos[s]);
+    dfree(c->arena, sp.force[s]);
     sp.pos[s] = nullptr;
     sp.force[s] = nullptr;
   }
   sp.cap = 0;
   for (int s = 0; s < 2; s++) {
-    CK(cudaMalloc(&sp.pos[s], sizeof(uint32_t) * 3 * np));
-    CK(cudaMalloc(&sp.force[s], sizeof(float) * 3 * np));
+    CK(dmalloc(c->arena, &sp.pos[s], sizeof(uint32_t) * 3 * np));
+    CK(dmalloc(c->arena, &sp.force[s], sizeof(float) * 3 * np));
   }
   sp.cap = np;
   return 0;
@@ -58,8 +58,8 @@ void tpm::free_stream_state(tpm_ctx *c) {
   if (sp.in) cudaStreamSynchronize(sp.in);
   if (sp.out) cudaStreamSynchronize(sp.out);
   for (int s = 0; s < 2; s++) {
-    if (sp.pos[s]) cudaFree(sp.pos[s]);
-    if (sp.force[s]) cudaFree(sp.force[s]);
+    dfree(c->arena, sp.pos[s]);
+    dfree(c->arena, sp.force[s]);
     if (sp.ev_in[s]) cudaEventDestroy(sp.ev_in[s]);
     if (sp.ev_comp[s]) cudaEventDestroy(sp.ev_comp[s]);
     if (sp.ev_out[s]) cudaEventDestroy(sp.ev_out[s]);

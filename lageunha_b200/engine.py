@@ -164,6 +164,7 @@ _SIGS = {
     "tpm_server_info": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(TpmRequestInfo)]),
     "tpm_server_wait": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double]),
     "tpm_server_stats": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tpm_server_reserve": (ctypes.c_int, [_P, ctypes.c_int64]),
     "tpm_server_destroy": (ctypes.c_int, [_P]),
     "tpm_evol_factors": (ctypes.c_int, [ctypes.POINTER(TpmCosmology), ctypes.c_int32, ctypes.c_float,
                                         ctypes.c_float, ctypes.POINTER(TpmEvolFact)]),
@@ -511,7 +512,7 @@ class Batch:
 
 
 SERVER_STATS = ("done", "failed", "peak_active", "peak_bytes", "contexts_created", "contexts_reused",
-                "contexts_evicted", "deferred_admissions")
+                "contexts_evicted", "deferred_admissions", "create_us", "upload_us", "capture_us", "reserve_us", "arena_bytes")
 
 
 def estimate_bytes(n_mesh: int, np_: int) -> int:
@@ -523,12 +524,19 @@ class Server:
     requests for boxes of different sizes on one device. Arrays handed to
     submit() are kept referenced here until the server is closed."""
 
-    def __init__(self, hbm_cap_bytes: int = 150 * 10 ** 9, max_active: int = 64, device: int = 0):
+    def __init__(self, hbm_cap_bytes: int = 150 * 10 ** 9, max_active: int = 64, device: int = 0,
+                 reserve_bytes: int = 0):
         self._lib = load_library()
         s = ctypes.c_void_p()
         _check(self._lib.tpm_server_create(device, int(hbm_cap_bytes), max_active, ctypes.byref(s)))
         self._s = s
         self._keep = {}
+        if reserve_bytes:
+            self.reserve(reserve_bytes)
+
+    def reserve(self, nbytes: int):
+        """Claims device memory for the contexts now (tpm_server_reserve)."""
+        _check(self._lib.tpm_server_reserve(self._s, int(nbytes)))
 
     def submit(self, pos, vel=None, *, n_mesh: int, nsteps: int = 0, anow: float = 1.0, astep: float = 0.0,
                cosmo: TpmCosmology | None = None, pos_out=None, vel_out=None, force_out=None, **params) -> int:
@@ -564,8 +572,8 @@ class Server:
         _check(self._lib.tpm_server_wait(self._s, rid, timeout))
 
     def stats(self) -> dict:
-        out = np.zeros(8, np.int64)
-        k = self._lib.tpm_server_stats(self._s, out.ctypes.data, 8)
+        out = np.zeros(len(SERVER_STATS), np.int64)
+        k = self._lib.tpm_server_stats(self._s, out.ctypes.data, len(SERVER_STATS))
         return {SERVER_STATS[i]: int(out[i]) for i in range(k)}
 
     def close(self):

@@ -122,3 +122,36 @@ def test_rejects_requests_above_the_cap():
             srv.submit(b.pos, b.vel, n_mesh=b.n_mesh, **KW)
         with pytest.raises(E.EngineError):
             srv.submit(b.pos, b.vel, n_mesh=8, **KW)  # mesh below the minimum
+
+
+def test_arena_memory_is_reused_across_mesh_sizes():
+    """Requests of different meshes, one after another under a cap that holds
+    about two contexts: idle contexts are evicted and their buffers go back to
+    the server's arena, which the next contexts draw from. The arena claims at
+    most one growth block beyond what was reserved up front, and the last
+    request's forces are the plain engine's."""
+    boxes = [_box(40 + i, nl, ic.fft_friendly(nl)) for i, nl in enumerate((48, 40, 56, 44, 52, 36, 60))]
+    need = max(E.estimate_bytes(b.n_mesh, b.np) for b in boxes)
+    cap = int(2.5 * need)
+    last = boxes[-1]
+    with E.Engine(last.n_mesh, **KW) as eng:
+        eng.load_fixed(last.pos, last.vel)
+        eng.compute(E.PART_ALL)
+        want = eng.forces()
+    fo = np.empty((last.np, 3), np.float32)
+    with E.Server(hbm_cap_bytes=cap, reserve_bytes=cap) as srv:
+        assert srv.stats()["arena_bytes"] >= cap
+        for b in boxes[:-1]:
+            srv.wait(srv.submit(b.pos, b.vel, n_mesh=b.n_mesh, nsteps=1, anow=4.0, astep=0.05, **KW))
+        srv.wait(srv.submit(last.pos, last.vel, n_mesh=last.n_mesh, force_out=fo, **KW))
+        st = srv.stats()
+    assert st["done"] == len(boxes) and st["failed"] == 0
+    assert st["contexts_evicted"] > 0
+    assert st["arena_bytes"] <= cap + (1 << 30)  # at most one 1 GiB growth block beyond the reserve
+    assert _close(fo, want, 1e-5)
+
+
+def test_reserve_above_the_cap_is_refused():
+    with E.Server(hbm_cap_bytes=10 ** 9) as srv:
+        with pytest.raises(E.EngineError):
+            srv.reserve(2 * 10 ** 9)
