@@ -787,6 +787,13 @@ def run_engine_arm(args):
                    "parallelism": f"replicas x{ws}"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "stage_ms": per,
+        # the PM chain (deposit, fft, fda4) runs on a second stream beside the
+        # tree build, so stage_ms' tree_build spans that whole phase (from the
+        # deposit's start to the tree's end) and the stages do not add up
+        "phase_ms": {"sort": per.get("sort", 0.0), "pm_chain_beside_tree_build": per.get("tree_build", 0.0),
+                     "tree_walk": per.get("tree_walk", 0.0),
+                     "finish_and_gaps": ms_step - per.get("sort", 0.0) - per.get("tree_build", 0.0)
+                     - per.get("tree_walk", 0.0)},
         "hbm_stages": hbm_stages,
         "counters": counters,
         "err_vs_ewald": err,
