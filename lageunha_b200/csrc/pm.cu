@@ -105,16 +105,21 @@ TPM_D void tsc_axis3(uint32_t u, uint32_t n, uint32_t half, float scale, float w
 // exactly. Integer sums do not depend on the order of the additions.
 TPM_D void fix_add(uint32_t *acc, int i, float v) { atomicAdd(&acc[i], __float2uint_rn(v)); }
 
-// Adds the 27 weights of every valid lane to acc, merging runs of lanes with
-// the same home node by a warp segmented sum first (dense clumps put many
-// particles on one node).
+// Adds the 27 weights of every valid lane to acc. When at least half of the
+// warp's lanes start a run of equal home nodes, every lane adds its own
+// weights (integer atomics to one address serialise, but a few repeats cost
+// less than merging); otherwise (dense clumps put many particles on one node)
+// the runs are merged by a warp segmented sum first. Measured: the 512^3
+// workload's deposit 5.53 -> 5.28 ms and the clustered 256^3 one 0.99 -> 0.93
+// ms against merging whenever any two lanes share a node; always adding
+// directly took 5.10 and 1.40 ms.
 TPM_D void deposit_lanes(uint32_t *acc, bool valid, int home, const float wx[3], const float wy[3],
                          const float wz[3], int lane) {
   int key = valid ? home : -1 - lane;
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
   bool head = lane == 0 || prev != key;
   unsigned heads = __ballot_sync(0xffffffffu, head);
-  if (heads == 0xffffffffu) {
+  if (__popc(heads) >= 16) {
     if (valid) {
       for (int c = 0; c < 3; c++)
         for (int b = 0; b < 3; b++)
