@@ -56,13 +56,16 @@ TPM_D Axis axis_of(uint32_t u, uint32_t n, uint32_t half = 0) {
   uint64_t p = (uint64_t)u * (uint64_t)n + (half ? 0x80000000ull : 0ull);
   int c = (int)(p >> 32);
   uint32_t fr = (uint32_t)p;
+  // xmin is the FP64 value fr 2^-32 (or fr 2^-32 - 1) rounded to float:
+  // both are a 32-bit integer times 2^-32, so rounding that integer to float
+  // and scaling by the power of two gives the same bits without FP64
   Axis a;
   if (fr > 0x80000000u) {
     a.near = c + 1;
-    a.xmin = (float)((double)fr * (1.0 / 4294967296.0) - 1.0);
+    a.xmin = -(__uint2float_rn(0u - fr) * 2.3283064365386963e-10f);
   } else {
     a.near = c;
-    a.xmin = (float)((double)fr * (1.0 / 4294967296.0));
+    a.xmin = __uint2float_rn(fr) * 2.3283064365386963e-10f;
   }
   return a;
 }
@@ -164,6 +167,14 @@ TPM_D void deposit_lanes(uint32_t *acc, bool valid, int home, const float wx[3],
   }
 }
 
+// v in [-n, 2n) into [0, n): the flush's node coordinates lie within a few
+// cells of the box (tile origin - 4 to + 12, n >= 16), so one conditional
+// add or subtract replaces an integer remainder by the run-time n.
+TPM_D int wrap_once(int v, int n) {
+  v += v < 0 ? n : 0;
+  return v >= n ? v - n : v;
+}
+
 // Adds a tile's shared-memory accumulator (origin ox = t-1 per axis) to the
 // periodic mesh. vec4: the mesh's x rows are added as float4 groups aligned
 // to 4 cells, [t-4, t), ..., [t+8, t+12), read from the accumulator with
@@ -183,10 +194,7 @@ TPM_D void flush_tile(const uint32_t *acc, float inv_scale, float *__restrict__ 
         v[j] = (xi >= 0 && xi < kUsed) ? (float)row[xi] * inv_scale : 0.f;
       }
       if (v[0] == 0.f && v[1] == 0.f && v[2] == 0.f && v[3] == 0.f) continue;
-      int gx = ox - 3 + 4 * q, gy = oy + y, gz = oz + z;
-      gx = (gx % n + n) % n;
-      gy = (gy % n + n) % n;
-      gz = (gz % n + n) % n;
+      int gx = wrap_once(ox - 3 + 4 * q, n), gy = wrap_once(oy + y, n), gz = wrap_once(oz + z, n);
       float4 *dst = reinterpret_cast<float4 *>(rho + gx + (int64_t)n * (gy + (int64_t)n * gz));
       atomicAdd(dst, make_float4(v[0], v[1], v[2], v[3]));
     }
@@ -196,7 +204,7 @@ TPM_D void flush_tile(const uint32_t *acc, float inv_scale, float *__restrict__ 
       int y = r % kUsed, z = r / kUsed;
       float v = (float)acc[x + kDepNx * (y + kDepNy * z)] * inv_scale;
       if (v == 0.f) continue;
-      int gx = ((ox + x) % n + n) % n, gy = ((oy + y) % n + n) % n, gz = ((oz + z) % n + n) % n;
+      int gx = wrap_once(ox + x, n), gy = wrap_once(oy + y, n), gz = wrap_once(oz + z, n);
       atomicAdd(rho + gx + (int64_t)n * (gy + (int64_t)n * gz), v);
     }
   }
