@@ -218,9 +218,11 @@ TPM_D uint32_t morton_compact(uint64_t x) {
 
 // Write the children of level-l nodes: node records of level l+1 in the
 // order of their parents, siblings contiguous in octant order.
+// q_to_frac = 1 / (2^sub_bits n): axis units of the key to fractions of the
+// box, so a cube centre is one FP64 multiply (no divisions per node).
 __global__ void __launch_bounds__(kBuildThreads) k_tree_write(const uint64_t *__restrict__ key,
                                                               TreeBuffers tb, int l, uint32_t n,
-                                                              int sub_bits) {
+                                                              int sub_bits, double q_to_frac) {
   uint32_t b = tb.level_range[2 * l], e = tb.level_range[2 * l + 1];
   uint32_t e1 = tb.level_range[2 * (l + 1) + 1];
   bool overflow = (e1 == e);  // capacity hit: nothing written below this level
@@ -253,8 +255,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_tree_write(const uint64_t *__
       uint32_t cu[3];
       for (int a = 0; a < 3; a++) {
         uint32_t qc = q[a] & ~(cside_q - 1u);
-        double cells = ((double)qc + 0.5 * (double)cside_q) / (double)(1u << sub_bits);
-        double fr = cells / (double)n;
+        double fr = ((double)qc + 0.5 * (double)cside_q) * q_to_frac;
         fr -= floor(fr);
         cu[a] = (uint32_t)(unsigned long long)llrint(fr * 4294967296.0);
       }
@@ -370,7 +371,8 @@ void tree_build(const TreeParams &tp, const uint64_t *key, const uint32_t *spos,
     k_tree_count<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l);
     k_tree_scan_chunks<<<kScanGrid, 1024, 0, st>>>(tb, l);
     k_tree_scan<<<1, 1024, 0, st>>>(tb, l, err);
-    k_tree_write<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l, tp.n, tp.sub_bits);
+    k_tree_write<<<kBuildGrid, kBuildThreads, 0, st>>>(key, tb, l, tp.n, tp.sub_bits,
+                                                       1.0 / ((double)(1u << tp.sub_bits) * (double)tp.n));
     nl += 4;
   }
   float inv_theta2 = 1.f / tp.theta2;
