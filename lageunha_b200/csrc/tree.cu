@@ -918,6 +918,7 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
     // particles. Nodes above that level are larger than the reach and would
     // only be opened.
     const int ncell = wl.box.n_cells;
+    const float inv_ncell = __frcp_rn((float)ncell);
     int srun[3][4];
     int stotal;
     {
@@ -944,7 +945,21 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
         sj += 32;
         if (j < stotal) {
           int nx = srun[0][1] + srun[0][3], ny = srun[1][1] + srun[1][3];
-          int jj[3] = {j % nx, (j / nx) % ny, j / (nx * ny)};
+          // j = jx + nx (jy + ny jz); below 2^20 the quotients come exact from
+          // float reciprocals ((q + 0.5) / d lies 0.5 / d from an integer,
+          // far above the float error), else from integer division
+          int jj[3];
+          if (stotal < (1 << 20)) {
+            int qx = (int)(((float)j + 0.5f) * __frcp_rn((float)nx));
+            int qy = (int)(((float)qx + 0.5f) * __frcp_rn((float)ny));
+            jj[0] = j - qx * nx;
+            jj[1] = qx - qy * ny;
+            jj[2] = qy;
+          } else {
+            jj[0] = j % nx;
+            jj[1] = (j / nx) % ny;
+            jj[2] = j / (nx * ny);
+          }
           const float gc[3] = {cx, cy, cz}, gh[3] = {hx, hy, hz};
           const uint32_t ur[3] = {w.rx, w.ry, w.rz};
           uint32_t cc[3];
@@ -957,7 +972,8 @@ __global__ void __launch_bounds__(kWalkThreads, kWalkBlocksPerSm) k_tree_walk(
             float c_lo = (float)(4 * c), c_hi = (float)min(4 * c + 4, ncell);
             float ref = __uint2float_rn(ur[a]) * wl.box.cpu;
             float d = 0.5f * (c_lo + c_hi) - (ref + gc[a]);
-            d -= (float)ncell * rintf(d / (float)ncell);
+            // minimum image (at exactly half a box both images are equally far)
+            d -= (float)ncell * rintf(d * inv_ncell);
             float e = fmaxf(fabsf(d) - 0.5f * (c_hi - c_lo) - gh[a], 0.f);
             d2 += e * e;
           }

@@ -99,3 +99,16 @@ def test_start_cube_runs_cover_the_reach_once():
             assert len(listed) == len(set(listed)), (n, lo, hi, runs)
             assert set(listed) >= _cubes_meeting(lo, hi, n), (n, lo, hi, runs)
             assert all(0 <= c < (n + 3) >> 2 for c in listed)
+
+
+def test_start_cube_index_split_by_float_reciprocal():
+    """The walk splits its start-cube index j = jx + nx (jy + ny jz) with float
+    reciprocals: q = int((j + 0.5) * rcp(d)). The product lies 0.5 / d from the
+    nearest integer and the float error is far below that, so q = j // d for
+    every j below 2^20 (the walk falls back to integer division above): here
+    every divisor up to 96 cubes per axis, IEEE float32 as the device rounds."""
+    j = np.arange(0, 1 << 20, dtype=np.int64)
+    jf = j.astype(np.float32) + np.float32(0.5)
+    for d in range(1, 97):
+        q = (jf * (np.float32(1) / np.float32(d))).astype(np.int64)
+        assert np.array_equal(q, j // d), d
