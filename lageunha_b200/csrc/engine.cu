@@ -165,10 +165,11 @@ static int build_law(tpm_ctx *c) {
       double r2 = s - (double)kLogR2Floor, r = std::max(sqrt(std::max(r2, 0.0)), 0.0009765625);
       v[k] = (r2 >= rs2 && !hard_cut) ? 0.0 : -(law_f(p.law, r, p.epsilon, p.rs_split, LL) / r);
     }
-    const double sc = (double)(1 << kLogMantissa);
     for (int k = 0; k < kLogEntries; k++) {
-      double d = (v[k + 1] - v[k]) * sc;
-      tlog[k] = make_float2((float)(v[k] - d), (float)d);
+      double s0 = at_bits((uint32_t)(kLogBase + k) << kLogShift);
+      double s1 = at_bits((uint32_t)(kLogBase + k + 1) << kLogShift);
+      double slope = (v[k + 1] - v[k]) / (s1 - s0);
+      tlog[k] = make_float2((float)(v[k] - slope * s0), (float)slope);
     }
     tlog[kLogEntries] = make_float2(0.f, 0.f);
     // the first entry from which the column is zero: the walk reads no entry

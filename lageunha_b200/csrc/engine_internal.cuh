@@ -190,10 +190,14 @@ void tree_groups(const TreeParams &tp, const uint64_t *key, int64_t np, TreeBuff
 // float bits of s = r^2 + kLogR2Floor (cells^2). Entry k covers
 // [s_k, s_{k+1}), s_k the float whose top bits are (kLogBase + k) <<
 // kLogShift: 2^kLogMantissa bins per octave from 2^-20 (= kLogR2Floor, so
-// every s lands in the table without a lower clamp) to 2^6 cells^2. With m
-// the float of s's in-bin mantissa bits under exponent 0 (m in [1, 1 +
-// 2^-kLogMantissa)), the column is c.x + c.y * m: c.y = (v_{k+1} - v_k) *
-// 2^kLogMantissa and c.x = v_k - c.y, v_k the value at r^2 = s_k - kLogR2Floor.
+// every s lands in the table without a lower clamp) to 2^6 cells^2. The
+// particle-pair column is linear in s inside each bin, c.x + c.y * s:
+// c.y = (v_{k+1} - v_k) / (s_{k+1} - s_k) and c.x = v_k - c.y s_k, v_k the
+// value at r^2 = s_k - kLogR2Floor (one multiply-add on s itself, no
+// extraction of the in-bin mantissa). The node columns (kPc*) are linear in
+// m, the float of s's in-bin mantissa bits under exponent 0 (m in [1, 1 +
+// 2^-kPcMantissa)): c.x + c.y m with c.y = (v_{k+1} - v_k) 2^kPcMantissa and
+// c.x = v_k - c.y.
 constexpr float kLogR2Floor = 9.5367431640625e-07f;  // 2^-20
 constexpr int kLogMantissa = 7;
 constexpr int kLogShift = 23 - kLogMantissa;

@@ -543,17 +543,15 @@ struct WalkCtx {
 
 // The law at s = r^2 + kLogR2Floor (cells^2) from the table indexed by the
 // float bits of s: the exponent and the top kLogMantissa mantissa bits pick
-// the bin, the remaining mantissa bits are the position inside it, so neither
-// a square root nor a conversion is needed, and s >= 2^-20 needs no lower
-// clamp. tlb is the table's shared address with the base entry kLogBase
-// folded in (s >= 2^-20 keeps the entry >= 0; the clamp keeps it in range).
+// the bin, whose line in s gives the value, so neither a square root nor a
+// conversion is needed, and s >= 2^-20 needs no lower clamp. tlb is the
+// table's shared address with the base entry kLogBase folded in (s >= 2^-20
+// keeps the entry >= 0; the clamp keeps it in range).
 TPM_D float law_at(float s, uint32_t tlb) {
-  uint32_t bits = __float_as_uint(s);
-  uint32_t kk = min(bits >> kLogShift, (uint32_t)(kLogBase + kLogEntries));
-  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
+  uint32_t kk = min(__float_as_uint(s) >> kLogShift, (uint32_t)(kLogBase + kLogEntries));
   float2 c;
   asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
-  return fmaf(c.y, m, c.x);
+  return fmaf(c.y, s, c.x);
 }
 
 // The law at s with every pair beyond the cut reading one shared entry: the
@@ -563,12 +561,10 @@ TPM_D float law_at(float s, uint32_t tlb) {
 // address, a broadcast, and the warp's gather spreads over the banks of the
 // pairs inside the cut only. Same value as law_at with the cut applied.
 TPM_D float law_clamped(float s, uint32_t tlb, uint32_t kcut) {
-  uint32_t bits = __float_as_uint(s);
-  uint32_t kk = min(bits >> kLogShift, kcut);
-  float m = __uint_as_float((bits & ((1u << kLogShift) - 1u)) | 0x3f800000u);
+  uint32_t kk = min(__float_as_uint(s) >> kLogShift, kcut);
   float2 c;
   asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(c.x), "=f"(c.y) : "r"(tlb + (kk << 3)));
-  return fmaf(c.y, m, c.x);
+  return fmaf(c.y, s, c.x);
 }
 
 // One source against this lane's target: the reference's AddPar
