@@ -138,13 +138,22 @@ def _ncu_traffic():
 
 
 # ---------------------------------------------------------------- CPU arms
-def reference_sample():
-    """The bounded CPU sample: the same clustered workload at 128^3 (2.1M
-    particles, 25 Plummer spheres of 2000-20000 particles with the same scale
-    radius, so the same local densities), one PM + tree-correction
-    evaluation through the reference's own pmmain/treecorrection."""
+SAMPLE_N = 128
+
+
+def reference_sample(workload):
+    """The bounded CPU sample: the benchmark's workload generated at 128^3
+    (2.1M particles; the 512^3 field's spectrum and displacement in lattice
+    units, or the clustered field's Plummer spheres with the same particle
+    counts and scale radius, so the same local densities), one PM +
+    tree-correction evaluation through the reference's own
+    pmmain/treecorrection."""
     from lageunha_b200 import ic
-    return ic.workload("clustered256", scale=128)
+    return ic.workload(workload, scale=SAMPLE_N)
+
+
+def sample_name(workload):
+    return f"{workload} workload at {SAMPLE_N}^3"
 
 
 def run_reference_eval(ps):
@@ -195,15 +204,15 @@ def run_ic(E, ic, n, local):
     return res
 
 
-def cpu_baseline():
-    ps = reference_sample()
+def cpu_baseline(workload):
+    ps = reference_sample(workload)
     saved = _quiet_stdout()
     try:
         dt = run_reference_eval(ps)
     finally:
         _restore_stdout(saved)
     return {"value": ps.np / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"clustered workload at 128^3 ({ps.np} particles, 25 Plummer spheres), one "
+            "sample": f"{sample_name(workload)} ({ps.np} particles), one "
                       f"pmmain + treecorrection of the reference built from its sources (variant A), "
                       f"OpenMP on {os.cpu_count()} host threads, {dt:.1f} s; its FFTs run on the harness's "
                       f"double-precision DFT (oracle/dft.c) in place of FFTW, which is not built",
@@ -235,7 +244,7 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_A.so was not built "
                           "(the reference tree was absent when the oracle was compiled)"}))
         return 0
-    ps = reference_sample()
+    ps = reference_sample(args.workload)
     saved = _quiet_stdout()
     try:
         for _ in range(args.warmup):
@@ -249,12 +258,14 @@ def run_reference_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded Zel'dovich + Plummer spheres)",
-        "config": {"workload": "clustered, bounded CPU sample at 128^3", "n_mesh": 128, "particles": ps.np,
+        "data": "synthetic (seeded Zel'dovich field" + (" + Plummer spheres" if args.workload == "clustered256" else "")
+                + "; no dataset)",
+        "config": {"workload": WORKLOADS[args.workload] + f"; bounded CPU sample: the same field at {SAMPLE_N}^3",
+                   "n_mesh": ps.n_mesh, "particles": ps.np,
                    "theta": 0.3, "rsphere": 4.0, "epsilon": EPS, "efold": 0.9},
         "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                         "sample": f"{ps.np} particles (clustered 128^3) per step, reference pmmain + "
+                         "sample": f"{ps.np} particles ({sample_name(args.workload)}) per step, reference pmmain + "
                                    f"treecorrection (variant A) on {os.cpu_count()} host threads; FFTs on "
                                    f"the harness's double-precision DFT (oracle/dft.c), not FFTW"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -556,15 +567,15 @@ def run_clustered(args, E, ic, local, dist=None):
     return out
 
 
-def parity_vs_reference(E, local):
-    """The engine with the reference's law on the CPU sample (clustered 128^3)
+def parity_vs_reference(E, local, workload):
+    """The engine with the reference's law on the CPU sample (the workload at 128^3)
     against the reference's own pmmain + treecorrection built from its
     sources (variant B, the three one-line fixes): per-particle relative
     force error, every particle."""
     from oracle import oracle as O
     if not O.ref_available(O.VARIANT_B):
         return {"unavailable": "oracle/_ref/libref_B.so was not built"}
-    ps = reference_sample()
+    ps = reference_sample(workload)
     with E.Engine(ps.n_mesh, epsilon=EPS, device=local, **REFERENCE_LAW) as eng:
         eng.load_fixed(ps.positions_u32())
         eng.compute(E.PART_ALL)
@@ -576,7 +587,7 @@ def parity_vs_reference(E, local):
     finally:
         _restore_stdout(saved)
     e = O.rel_err(f, fr)
-    return {"sample": f"clustered workload at 128^3, {ps.np} particles, reference law (theta 0.3, rsphere 4)",
+    return {"sample": f"{sample_name(workload)}, {ps.np} particles, reference law (theta 0.3, rsphere 4)",
             "oracle": "reference pmmain + treecorrection built from its sources (variant B)",
             "rms": float(np.sqrt(np.mean(e * e))), "p99": float(np.percentile(e, 99)), "particles": ps.np}
 
@@ -855,8 +866,8 @@ def run_engine_arm(args):
     if not args.no_served:
         line["served"] = {"law": box_law, **run_served(args, E, ic, box_law, local, dist)}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
-        line["parity_vs_reference"] = parity_vs_reference(E, local)
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+        line["parity_vs_reference"] = parity_vs_reference(E, local, args.workload)
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
