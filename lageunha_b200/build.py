@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtpm_engine.so")
 SOURCES = ["engine.cu", "arena.cu", "sort.cu", "pm.cu", "tree.cu", "ewald.cu", "noalloc.cu", "step.cu", "batch.cu", "server.cu", "tune.cu", "snapshot.cpp", "spectrum.cu", "fof.cu", "ic.cu", "stream.cu"]
-HEADERS = ["common.cuh", "engine_internal.cuh", "ctx.cuh"]
+HEADERS = ["arena_core.h", "common.cuh", "engine_internal.cuh", "ctx.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
